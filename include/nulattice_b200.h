@@ -1,0 +1,154 @@
+/*
+ * nulattice_b200 -- C ABI of the B200 CCSD kernels.
+ *
+ * The reference (NuLattice) is pure Python and has no FFI: its CCSD entry
+ * point is the Python function `ccsd_solver` (CCM/coupled_cluster.py:547-687,
+ * torch twin CCM/soa/coupled_cluster.py:440-575).  The Python package
+ * `nulattice_b200` mirrors that function and calls the entry points below
+ * through ctypes; every comment names the reference code whose work the
+ * entry point takes over.
+ *
+ * Conventions
+ *  - Every pointer is a device pointer unless its name ends in `_host`.
+ *  - No entry point allocates device memory: the caller owns every buffer
+ *    (sizes from the *_bytes queries).  The stream is the caller's.
+ *  - Return value: NLB_OK (0) or a positive NLB_ERR_* code; launches are
+ *    asynchronous, so a kernel fault surfaces at the caller's next sync.
+ *  - Amplitudes are stored either as FP64 or FP32 (`dtype` = NLB_F64 /
+ *    NLB_F32); T1, the energy, norms and the DIIS algebra are always FP64.
+ */
+#ifndef NULATTICE_B200_H
+#define NULATTICE_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *nlb_stream_t; /* a cudaStream_t */
+
+enum { NLB_OK = 0, NLB_ERR_ARG = 1, NLB_ERR_LAUNCH = 2, NLB_ERR_SIZE = 3, NLB_ERR_CUDA = 4 };
+enum { NLB_F64 = 0, NLB_F32 = 1 };
+enum { NLB_RUNNING = 0, NLB_CONVERGED = 1, NLB_MAX_ITER = 2, NLB_DIVERGED = 3 };
+enum { NLB_CRIT_SOA = 0, NLB_CRIT_NUMPY = 1 };
+
+/* One channel (label pair g1 < g2) of the compact T2: a dense block
+ * B[a'][b'][i'][j'] of np1*np2*nh1*nh2 numbers at element `offset`. */
+typedef struct {
+    int32_t g1, g2, np1, np2, nh1, nh2;
+    int32_t pb1, pb2, hb1, hb2;   /* label bases into p_ord / h_ord */
+    int64_t offset;               /* element offset in compact T2 */
+    int64_t gb_off, ga_off;       /* element offsets of the G intermediates */
+    int64_t hh_ptr_off, hh_col_off, pp_ptr_off, pp_col_off;
+} nlb_channel;
+
+/* Structured problem description (closed-site, label-conserving inputs).
+ * Built on the host by nulattice_b200.structure; all arrays on the device. */
+typedef struct {
+    int32_t p, h, n_labels, n_channels;
+    int64_t n_t2;                 /* compact T2 length */
+    int64_t n_g;                  /* G-intermediate length */
+    const nlb_channel *chan;      /* [n_channels] */
+    const int64_t *t2_end;        /* [n_channels] cumulative end of each block */
+    const int64_t *g_end;         /* [n_channels] cumulative end of G items */
+    const int32_t *p_ord;         /* [p] particle index of label-ordered row */
+    const int32_t *h_ord;         /* [h] */
+    const int32_t *p_label, *h_label, *p_loc, *h_loc;   /* [p], [h], [p], [h] */
+    const int32_t *p_base, *h_base;                     /* [n_labels+1] */
+    const int32_t *fpp_ptr, *fpp_col; const double *fpp_val;  /* f_pp CSR per label */
+    const double *fpp_diag;       /* [p] */
+    const int32_t *fph_ptr, *fph_col; const double *fph_val;  /* f_ph per hole */
+    const double *f_ph;           /* [p*h] dense */
+    const double *f_hh;           /* [h*h] dense */
+    const int32_t *hh_ptr, *hh_col; const double *hh_val;     /* hole-hole ladder CSR */
+    const int32_t *pp_ptr, *pp_col; const double *pp_val;     /* particle-particle ladder CSR */
+} nlb_struct_problem;
+
+/* Device-resident solver state shared by the kernels of one solve. */
+typedef struct {
+    double e_acc;       /* energy of the amplitudes being written */
+    double dt1_sq;      /* ||t1_new - t1||^2 */
+    double dt2_sq;      /* ||t2_new - t2||^2 (dense weight applied) */
+    double e_prev;      /* energy of the previous step */
+    double e_last;      /* energy of the last finished step */
+    double eps;
+    double mixing;
+    double gram[121];   /* DIIS Gram matrix (max_diis <= 10), then coefficients */
+    int32_t parity;     /* which amplitude buffer is current */
+    int32_t iter;
+    int32_t status;
+    int32_t max_steps;
+    int32_t criterion;  /* NLB_CRIT_SOA / NLB_CRIT_NUMPY */
+    int32_t max_diis;
+    int32_t diis_count; /* error vectors stored since the last extrapolation */
+    int32_t diis_pulse; /* 1 when the step just finished must extrapolate */
+    int32_t diis_applied;
+    int32_t ccs;
+} nlb_ctrl;
+
+/* Per-solve buffers (all caller-allocated). */
+typedef struct {
+    double *t1[2];      /* [p*h] double-buffered T1 */
+    void *t2[2];        /* [n_t2] double-buffered compact T2 (dtype) */
+    void *g;            /* [n_g] G intermediates (dtype) */
+    double *prep;       /* [nlb_struct_prep_len(p,h)] dressed-Fock scratch */
+    double *diis_t1;    /* [max_diis * p*h] T1 error ring (may be NULL) */
+    void *diis_t2;      /* [max_diis * n_t2] T2 error ring (dtype, may be NULL) */
+    nlb_ctrl *ctrl;
+    int32_t dtype;
+} nlb_struct_state;
+
+int nlb_version(void);
+/* human-readable text of the last error set on the calling host thread */
+const char *nlb_last_error(void);
+
+/* Length (doubles) of the dressed-Fock scratch: Q, X_hh (T2 eq), X_hh (T1 eq)
+ * as h*h each, and the particle diagonals of X_pp for both equations. */
+int64_t nlb_struct_prep_len(int32_t p, int32_t h);
+
+/* Reset `ctrl` on the device and load the solver parameters. */
+int nlb_struct_ctrl_init(nlb_ctrl *ctrl, double eps, double mixing, int32_t max_steps,
+                         int32_t criterion, int32_t max_diis, int32_t ccs, double e0,
+                         nlb_stream_t stream);
+
+/* One CCSD Jacobi step on the compact layout, replacing the reference's
+ * t1Iter + t2Iter + mixing + ccsd_energy (CCM/coupled_cluster.py:342-545,
+ * 614-623; ccDgrams.py terms that survive for closed-site inputs), followed by
+ * the convergence test (coupled_cluster.py:629 / soa/coupled_cluster.py:517).
+ * Reads the current buffers (ctrl->parity), writes the other ones, stores the
+ * DIIS error vectors when max_diis > 0 and flips ctrl->parity.  Kernels do
+ * nothing once ctrl->status != NLB_RUNNING, so steps may be queued ahead. */
+int nlb_struct_step(const nlb_struct_problem *prob, const nlb_struct_state *st,
+                    nlb_stream_t stream);
+
+/* Pulsed DIIS of the torch solver (CCM/soa/coupled_cluster.py:522-567): when
+ * ctrl->diis_pulse is set, build the Gram matrix of the stored error vectors
+ * (FP64), solve the bordered system in FP64 on the device and extrapolate the
+ * current amplitudes in place.  No-op otherwise. */
+int nlb_struct_diis(const nlb_struct_problem *prob, const nlb_struct_state *st,
+                    nlb_stream_t stream);
+
+/* Energy of the current amplitudes, sum_ai f_ai t1_ai (ccsd_energy,
+ * coupled_cluster.py:265-286, with v_pphh = 0), written to *e_out (device). */
+int nlb_struct_energy(const nlb_struct_problem *prob, const nlb_struct_state *st,
+                      double *e_out, nlb_stream_t stream);
+
+/* Copy between compact T2 of one dtype and another (FP32 <-> FP64). */
+int nlb_convert(const void *src, int32_t src_dtype, void *dst, int32_t dst_dtype,
+                int64_t n, nlb_stream_t stream);
+
+/* Scatter the compact T2 into the dense reference layout t2[a,b,i,j]
+ * (FP64, p*p*h*h, zero-filled by the caller) with all four antisymmetric
+ * images, and gather dense -> compact. */
+int nlb_struct_unpack_t2(const nlb_struct_problem *prob, const void *t2c, int32_t dtype,
+                         double *t2_dense, nlb_stream_t stream);
+int nlb_struct_pack_t2(const nlb_struct_problem *prob, const double *t2_dense, void *t2c,
+                       int32_t dtype, nlb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NULATTICE_B200_H */

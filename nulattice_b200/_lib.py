@@ -1,0 +1,102 @@
+"""ctypes binding of the C ABI declared in ``include/nulattice_b200.h``.
+
+The shared library is built in-tree (``nulattice_b200/_nlb_ccsd.so``) by
+``nulattice_b200.build``.  There is no fallback: if the library is missing or
+fails to load, every solver entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_nlb_ccsd.so")
+
+NLB_OK, NLB_ERR_ARG, NLB_ERR_LAUNCH, NLB_ERR_SIZE, NLB_ERR_CUDA = 0, 1, 2, 3, 4
+NLB_F64, NLB_F32 = 0, 1
+NLB_RUNNING, NLB_CONVERGED, NLB_MAX_ITER, NLB_DIVERGED = 0, 1, 2, 3
+NLB_CRIT_SOA, NLB_CRIT_NUMPY = 0, 1
+MAX_DIIS = 10
+
+c_int32, c_int64, c_double, c_void_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+# numpy mirror of nlb_channel (device array of channel descriptors)
+CHANNEL_DTYPE = np.dtype([(n, np.int32) for n in ("g1", "g2", "np1", "np2", "nh1", "nh2",
+                                                  "pb1", "pb2", "hb1", "hb2")] +
+                         [(n, np.int64) for n in ("offset", "gb_off", "ga_off", "hh_ptr_off",
+                                                  "hh_col_off", "pp_ptr_off", "pp_col_off")])
+assert CHANNEL_DTYPE.itemsize == 96
+
+
+class StructProblem(ctypes.Structure):
+    _fields_ = [("p", c_int32), ("h", c_int32), ("n_labels", c_int32), ("n_channels", c_int32),
+                ("n_t2", c_int64), ("n_g", c_int64)] + [
+        (n, c_void_p) for n in ("chan", "t2_end", "g_end", "p_ord", "h_ord", "p_label", "h_label",
+                                "p_loc", "h_loc", "p_base", "h_base", "fpp_ptr", "fpp_col", "fpp_val",
+                                "fpp_diag", "fph_ptr", "fph_col", "fph_val", "f_ph", "f_hh",
+                                "hh_ptr", "hh_col", "hh_val", "pp_ptr", "pp_col", "pp_val")]
+
+
+class Ctrl(ctypes.Structure):
+    _fields_ = [(n, c_double) for n in ("e_acc", "dt1_sq", "dt2_sq", "e_prev", "e_last", "eps", "mixing")] + \
+               [("gram", c_double * 121)] + \
+               [(n, c_int32) for n in ("parity", "iter", "status", "max_steps", "criterion", "max_diis",
+                                       "diis_count", "diis_pulse", "diis_applied", "ccs")]
+
+
+class StructState(ctypes.Structure):
+    _fields_ = [("t1", c_void_p * 2), ("t2", c_void_p * 2), ("g", c_void_p), ("prep", c_void_p),
+                ("diis_t1", c_void_p), ("diis_t2", c_void_p), ("ctrl", c_void_p), ("dtype", c_int32)]
+
+
+_lib = None
+_load_error = None
+
+
+def lib():
+    """The loaded library; raises RuntimeError when it is unavailable."""
+    global _lib, _load_error
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"nulattice_b200 CUDA library not built ({LIB_PATH} missing); "
+                           "run nulattice_b200.build.build()")
+    try:
+        L = ctypes.CDLL(LIB_PATH)
+    except OSError as e:  # pragma: no cover - depends on the machine
+        _load_error = str(e)
+        raise RuntimeError(f"cannot load {LIB_PATH}: {e}") from e
+    L.nlb_version.restype = c_int32
+    L.nlb_last_error.restype = ctypes.c_char_p
+    L.nlb_struct_prep_len.restype = c_int64
+    L.nlb_struct_prep_len.argtypes = [c_int32, c_int32]
+    L.nlb_struct_ctrl_init.argtypes = [c_void_p, c_double, c_double, c_int32, c_int32, c_int32, c_int32,
+                                       c_double, c_void_p]
+    for name in ("nlb_struct_step", "nlb_struct_diis"):
+        getattr(L, name).argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_void_p]
+    L.nlb_struct_energy.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_void_p,
+                                    c_void_p]
+    L.nlb_convert.argtypes = [c_void_p, c_int32, c_void_p, c_int32, c_int64, c_void_p]
+    L.nlb_struct_unpack_t2.argtypes = [ctypes.POINTER(StructProblem), c_void_p, c_int32, c_void_p, c_void_p]
+    L.nlb_struct_pack_t2.argtypes = [ctypes.POINTER(StructProblem), c_void_p, c_void_p, c_int32, c_void_p]
+    for name in ("nlb_struct_ctrl_init", "nlb_struct_step", "nlb_struct_diis", "nlb_struct_energy",
+                 "nlb_convert", "nlb_struct_unpack_t2", "nlb_struct_pack_t2"):
+        getattr(L, name).restype = c_int32
+    _lib = L
+    return L
+
+
+def check(rc, what=""):
+    if rc != NLB_OK:
+        msg = lib().nlb_last_error().decode(errors="replace")
+        raise RuntimeError(f"nulattice_b200 {what} failed (code {rc}): {msg}")
+
+
+def exported_symbols():
+    """Names declared in include/nulattice_b200.h (checked by the tests)."""
+    hdr = os.path.join(os.path.dirname(HERE), "include", "nulattice_b200.h")
+    import re
+    txt = open(hdr).read()
+    return sorted(set(re.findall(r"\b(nlb_[a-z0-9_]+)\s*\(", txt)))

@@ -1,0 +1,348 @@
+"""Drop-in CCSD solver: ``ccsd_solver`` with the reference's arguments.
+
+Mirrors ``NuLattice.CCM.soa.coupled_cluster.ccsd_solver``
+(``CCM/soa/coupled_cluster.py:440-575``; NumPy twin
+``CCM/coupled_cluster.py:547-687``): same positional and keyword arguments,
+same return value ``(E_corr, t1, t2)`` with ``t1[a,i]`` and
+``t2[a,b,i,j]`` in the reference layout.  The work runs in hand-written
+sm_100a kernels (``nulattice_b200/csrc``) reached through the C ABI of
+``include/nulattice_b200.h``; there is no CPU path.
+
+Two engines sit behind the entry point:
+
+* the *structured* engine, for inputs that conserve a label on every state
+  with closed hole sites (every lattice configuration of the examples): T2 is
+  kept in the compact channel layout of :mod:`nulattice_b200.structure`;
+* the *general* engine (:mod:`nulattice_b200.dense`), for anything else: the
+  full factorised equation set on dense tensors.
+
+Extra keyword-only arguments (not in the reference):
+
+``precision``  ``"fp64"`` (default) or ``"mixed"`` -- the structured engine
+               stores T2 in FP32 and computes the elementwise work in FP32
+               (T1, energies, norms and DIIS stay FP64), then finishes with
+               FP64 steps until ``eps`` is met.
+``criterion``  ``"soa"`` (default: ``|dE|/max(1,|E|) < eps`` and pulsed DIIS,
+               as the torch solver) or ``"numpy"`` (``|dE|/|E| < eps``, no
+               DIIS, as the NumPy solver whose DIIS branch never fires).
+``t2_format``  ``"dense"`` (default, reference layout) or ``"compact"``.
+``info``       a dict to fill with status, iterations, engine and timings.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import structure as _structure
+
+_CRIT = {"soa": _lib.NLB_CRIT_SOA, "numpy": _lib.NLB_CRIT_NUMPY}
+_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "diverged"}
+
+
+def _np(x):
+    if isinstance(x, torch.Tensor):
+        return x.detach().cpu().numpy()
+    if hasattr(x, "to_dense") and not isinstance(x, np.ndarray):
+        return np.asarray(x.to_dense())
+    return np.asarray(x)
+
+
+def _stream_ptr(dev):
+    return ctypes_void(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def ctypes_void(v):
+    import ctypes
+    return ctypes.c_void_p(v)
+
+
+def _resolve_device(device):
+    if device is None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("nulattice_b200.ccsd_solver needs a CUDA device (none available)")
+        return torch.device("cuda", torch.cuda.current_device())
+    dev = torch.device(device)
+    if dev.type != "cuda":
+        raise RuntimeError(f"nulattice_b200.ccsd_solver runs on CUDA devices only, got {dev}")
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    return dev
+
+
+class StructuredEngine:
+    """Device tables and buffers of one structured problem.
+
+    Building it uploads the channel plan once; :meth:`solve` can then be
+    called repeatedly (different initial amplitudes, precision, tolerances).
+    """
+
+    def __init__(self, plan, fock_mats, device):
+        self.plan = plan
+        self.dev = device
+        f_pp, f_ph, f_hh = [np.asarray(_np(f), dtype=np.float64) for f in fock_mats]
+        self.f_ph_np = f_ph
+        self.f_pp_np, self.f_hh_np = f_pp, f_hh
+        pl = plan
+        G = pl.n_labels
+        dev = device
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
+        i64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=dev)  # noqa: E731
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
+        p_ord = np.concatenate([pl.p_of[g] for g in range(G)]).astype(np.int32)
+        h_ord = np.concatenate([pl.h_of[g] for g in range(G)]).astype(np.int32)
+        chans = np.zeros(max(len(pl.channels), 1), dtype=_lib.CHANNEL_DTYPE)
+        t2_end, g_end = [], []
+        hh_ptr, hh_col, hh_val, pp_ptr, pp_col, pp_val = [], [], [], [], [], []
+        goff = hp_off = hc_off = pp_off = pc_off = 0
+        for n, ch in enumerate(pl.channels):
+            nhp = ch.nh1 * ch.nh2
+            n_gb = ch.np1 * ch.nh2 * nhp
+            n_ga = ch.np2 * ch.nh1 * nhp
+            chans[n] = (ch.g1, ch.g2, ch.np1, ch.np2, ch.nh1, ch.nh2,
+                        pl.p_base[ch.g1], pl.p_base[ch.g2], pl.h_base[ch.g1], pl.h_base[ch.g2],
+                        ch.offset, goff, goff + n_gb, hp_off, hc_off, pp_off, pc_off)
+            goff += n_gb + n_ga
+            t2_end.append(ch.offset + ch.size)
+            g_end.append(goff)
+            hh_ptr.append(pl.hh_ptr[n]); hh_col.append(pl.hh_col[n]); hh_val.append(pl.hh_val[n])
+            pp_ptr.append(pl.pp_ptr[n]); pp_col.append(pl.pp_col[n]); pp_val.append(pl.pp_val[n])
+            hp_off += len(pl.hh_ptr[n]); hc_off += len(pl.hh_col[n])
+            pp_off += len(pl.pp_ptr[n]); pc_off += len(pl.pp_col[n])
+        self.n_g = goff
+        cat = lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(1, dt)  # noqa: E731
+        T = {}
+        T["chan"] = torch.as_tensor(chans.view(np.uint8), device=dev)
+        T["t2_end"] = i64(t2_end or [0]); T["g_end"] = i64(g_end or [0])
+        T["p_ord"] = i32(p_ord); T["h_ord"] = i32(h_ord)
+        T["p_label"] = i32(pl.p_label); T["h_label"] = i32(pl.h_label)
+        T["p_loc"] = i32(pl.p_loc); T["h_loc"] = i32(pl.h_loc)
+        T["p_base"] = i32(pl.p_base); T["h_base"] = i32(pl.h_base)
+        T["fpp_ptr"] = i32(pl.fpp_ptr); T["fpp_col"] = i32(pl.fpp_col if len(pl.fpp_col) else [0])
+        T["fpp_val"] = f64(pl.fpp_val if len(pl.fpp_val) else [0.0]); T["fpp_diag"] = f64(np.diag(f_pp))
+        T["fph_ptr"] = i32(pl.fph_ptr); T["fph_col"] = i32(pl.fph_col if len(pl.fph_col) else [0])
+        T["fph_val"] = f64(pl.fph_val if len(pl.fph_val) else [0.0])
+        T["f_ph"] = f64(f_ph); T["f_hh"] = f64(f_hh)
+        T["hh_ptr"] = i32(cat(hh_ptr, np.int32)); T["hh_col"] = i32(cat(hh_col, np.int32))
+        T["hh_val"] = f64(cat(hh_val, np.float64))
+        T["pp_ptr"] = i32(cat(pp_ptr, np.int32)); T["pp_col"] = i32(cat(pp_col, np.int32))
+        T["pp_val"] = f64(cat(pp_val, np.float64))
+        self.tables = T
+        prob = _lib.StructProblem()
+        prob.p, prob.h, prob.n_labels, prob.n_channels = pl.p, pl.h, G, len(pl.channels)
+        prob.n_t2, prob.n_g = pl.n_t2, self.n_g
+        for k, v in T.items():
+            setattr(prob, k, v.data_ptr())
+        self.prob = prob
+        self._bufs = {}
+
+    # -- buffers ---------------------------------------------------------
+    def buffers(self, dtype_code, max_diis):
+        key = (dtype_code, max_diis)
+        if key in self._bufs:
+            return self._bufs[key]
+        pl, dev = self.plan, self.dev
+        tdt = torch.float64 if dtype_code == _lib.NLB_F64 else torch.float32
+        L = _lib.lib()
+        b = dict(
+            t1=[torch.zeros(pl.p * pl.h, dtype=torch.float64, device=dev) for _ in range(2)],
+            t2=[torch.zeros(max(pl.n_t2, 1), dtype=tdt, device=dev) for _ in range(2)],
+            g=torch.zeros(max(self.n_g, 1), dtype=tdt, device=dev),
+            prep=torch.zeros(int(L.nlb_struct_prep_len(pl.p, pl.h)), dtype=torch.float64, device=dev),
+            ctrl=torch.zeros(ctypes_sizeof_ctrl(), dtype=torch.uint8, device=dev),
+            diis_t1=torch.zeros(max(max_diis, 1) * pl.p * pl.h, dtype=torch.float64, device=dev)
+            if max_diis else None,
+            diis_t2=torch.zeros(max(max_diis, 1) * max(pl.n_t2, 1), dtype=tdt, device=dev)
+            if max_diis else None,
+        )
+        st = _lib.StructState()
+        st.t1[0], st.t1[1] = b["t1"][0].data_ptr(), b["t1"][1].data_ptr()
+        st.t2[0], st.t2[1] = b["t2"][0].data_ptr(), b["t2"][1].data_ptr()
+        st.g, st.prep, st.ctrl = b["g"].data_ptr(), b["prep"].data_ptr(), b["ctrl"].data_ptr()
+        st.diis_t1 = b["diis_t1"].data_ptr() if max_diis else None
+        st.diis_t2 = b["diis_t2"].data_ptr() if max_diis else None
+        st.dtype = dtype_code
+        b["state"] = st
+        self._bufs[key] = b
+        return b
+
+    def read_ctrl(self, b):
+        raw = b["ctrl"].cpu().numpy().tobytes()
+        return _lib.Ctrl.from_buffer_copy(raw)
+
+    # -- one phase of iterations ------------------------------------------
+    def run(self, b, t1_init, t2c_init, e0, eps, mixing, max_steps, criterion, max_diis, ccs,
+            verbose=False, sync_every=16, step_offset=0):
+        L = _lib.lib()
+        dev = self.dev
+        stream = torch.cuda.current_stream(dev)
+        sp = ctypes_void(stream.cuda_stream)
+        b["t1"][0].copy_(t1_init.reshape(-1))
+        if t2c_init is None:
+            b["t2"][0].zero_()
+        elif t2c_init.data_ptr() != b["t2"][0].data_ptr():
+            b["t2"][0].copy_(t2c_init)
+        b["t2"][1].zero_()
+        b["g"].zero_()
+        st = b["state"]
+        _lib.check(L.nlb_struct_ctrl_init(b["ctrl"].data_ptr(), eps, mixing, max_steps, criterion,
+                                          max_diis, int(bool(ccs)), e0, sp), "ctrl_init")
+        use_diis = max_diis > 0 and criterion == _lib.NLB_CRIT_SOA
+        done = 0
+        prev = e0
+        while done < max_steps:
+            n = 1 if verbose else min(sync_every, max_steps - done)
+            for _ in range(n):
+                _lib.check(L.nlb_struct_step(self.prob, st, sp), "step")
+                done += 1
+                if use_diis and done % max_diis == 0:
+                    _lib.check(L.nlb_struct_diis(self.prob, st, sp), "diis")
+            c = self.read_ctrl(b)
+            if verbose:
+                e = c.e_last
+                diff = abs(e - prev) / abs(e) if e != 0 else float("inf")
+                print(f"Step {step_offset + c.iter}: {e}", "difference =", diff)
+                prev = e
+            if c.status != _lib.NLB_RUNNING:
+                break
+        c = self.read_ctrl(b)
+        return c
+
+
+def ctypes_sizeof_ctrl():
+    import ctypes
+    return ctypes.sizeof(_lib.Ctrl)
+
+
+def _mp2_t1(f_pp, f_ph, f_hh, delta):
+    """``t1Init`` (``CCM/coupled_cluster.py:319-340``)."""
+    den = np.add.outer(-np.diag(f_pp), np.diag(f_hh)) + delta
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return f_ph / den
+
+
+def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10,
+                delta=0, mixing=0.5, verbose=False, sparse=True, ccs=False, device=None,
+                dtype=torch.float64, *, precision="fp64", criterion="soa", t2_format="dense",
+                mixed_eps=None, info=None):
+    """Solve the CCSD equations; returns ``(E_corr, t1, t2)``.
+
+    Arguments as ``CCM/soa/coupled_cluster.py:440-454``: ``fock_mats`` =
+    ``[f_pp, f_ph, f_hh]``; ``two_body_int`` = ``[v_pppp, v_ppph, v_pphh,
+    v_phph, v_phhh, v_hhhh]`` where ``v_pppp``/``v_ppph`` may be dense arrays,
+    ``[a,b,c,d,val]`` row lists, ``(indices, values)`` pairs or objects with
+    ``.indices``/``.values`` (repeated keys are summed), and the other blocks
+    dense arrays or such sparse objects.  ``sparse`` is accepted for
+    compatibility; the form of each block is detected.
+
+    Returns torch tensors on ``device`` when ``f_pp`` is a torch tensor, numpy
+    arrays otherwise.  On divergence the last amplitudes are returned (the
+    NumPy reference returns None there) and ``info["status"]`` says
+    ``"diverged"``.
+    """
+    t_start = time.perf_counter()
+    dev = _resolve_device(device)
+    if criterion not in _CRIT:
+        raise ValueError("criterion must be 'soa' or 'numpy'")
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("precision must be 'fp64' or 'mixed'")
+    if max_diis > _lib.MAX_DIIS:
+        raise ValueError(f"max_diis must be <= {_lib.MAX_DIIS}")
+    if not (0.0 <= float(mixing) <= 1.0):
+        raise ValueError("mixing must be in [0, 1]")
+    want_torch = isinstance(fock_mats[0], torch.Tensor)
+    _lib.lib()  # fail loudly before any work when the library is missing
+    plan, why = _structure.detect(fock_mats, two_body_int, t1initial)
+    if info is None:
+        info = {}
+    info["t_setup_start"] = t_start
+    if plan is None:
+        from . import dense as _dense
+        info["engine"] = "general"
+        info["why_general"] = why
+        e, t1, t2 = _dense.solve(fock_mats, two_body_int, t1initial=t1initial, eps=eps, maxSteps=maxSteps,
+                                 max_diis=max_diis, delta=delta, mixing=mixing, verbose=verbose, ccs=ccs,
+                                 device=dev, criterion=criterion, info=info)
+    else:
+        info["engine"] = "structured"
+        eng = StructuredEngine(plan, fock_mats, dev)
+        e, t1, t2 = solve_structured(eng, t1initial=t1initial, eps=eps, maxSteps=maxSteps,
+                                     max_diis=max_diis, delta=delta, mixing=mixing, verbose=verbose,
+                                     ccs=ccs, criterion=criterion, precision=precision,
+                                     t2_format=t2_format, mixed_eps=mixed_eps, info=info)
+    if info.get("status") == "max_iter":
+        print("Max iterations reached.")
+    elif info.get("status") == "diverged":
+        print("Diverged.")
+    if want_torch:
+        t1 = t1.to(dtype)
+        t2 = t2.to(dtype) if t2 is not None else t2
+    else:
+        t1 = t1.cpu().numpy()
+        t2 = t2.cpu().numpy() if t2 is not None else t2
+    info["t_total"] = time.perf_counter() - t_start
+    return e, t1, t2
+
+
+def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5,
+                     verbose=False, ccs=False, criterion="soa", precision="fp64", t2_format="dense",
+                     mixed_eps=None, info=None, sync_every=16):
+    """Run the structured engine (already built); see :func:`ccsd_solver`."""
+    info = {} if info is None else info
+    L = _lib.lib()
+    pl, dev = eng.plan, eng.dev
+    crit = _CRIT[criterion]
+    if t1initial is None:
+        t1 = _mp2_t1(eng.f_pp_np, eng.f_ph_np, eng.f_hh_np, float(delta))
+    else:
+        t1 = np.asarray(_np(t1initial), dtype=np.float64)
+    e0 = float(np.sum(eng.f_ph_np * t1))
+    t1_dev = torch.as_tensor(np.ascontiguousarray(t1), device=dev)
+    diis = int(max_diis) if crit == _lib.NLB_CRIT_SOA else 0
+    sp = ctypes_void(torch.cuda.current_stream(dev).cuda_stream)
+    iters = 0
+    t0 = time.perf_counter()
+    if precision == "mixed":
+        b32 = eng.buffers(_lib.NLB_F32, diis)
+        me = float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)
+        c = eng.run(b32, t1_dev, None, e0, me, mixing, maxSteps, crit, diis, ccs, verbose, sync_every)
+        iters += c.iter
+        info["mixed_iters"] = c.iter
+        info["mixed_energy"] = c.e_last
+        status = _STATUS[c.status]
+        if status == "converged" and c.e_last == c.e_last and maxSteps - iters > 0:
+            # continue in FP64 from the FP32 amplitudes
+            b64 = eng.buffers(_lib.NLB_F64, diis)
+            cur = c.parity
+            _lib.check(L.nlb_convert(b32["t2"][cur].data_ptr(), _lib.NLB_F32, b64["t2"][0].data_ptr(),
+                                     _lib.NLB_F64, pl.n_t2, sp), "convert")
+            c = eng.run(b64, b32["t1"][cur].clone(), b64["t2"][0], c.e_last, eps, mixing, maxSteps - iters,
+                        crit, diis, ccs, verbose, sync_every, step_offset=iters)
+            iters += c.iter
+            info["refine_iters"] = c.iter
+            b = b64
+        else:
+            b = b32
+    else:
+        b = eng.buffers(_lib.NLB_F64, diis)
+        c = eng.run(b, t1_dev, None, e0, eps, mixing, maxSteps, crit, diis, ccs, verbose, sync_every)
+        iters += c.iter
+    torch.cuda.current_stream(dev).synchronize()
+    info["t_iterate"] = time.perf_counter() - t0
+    info["status"] = _STATUS[c.status]
+    info["iterations"] = iters
+    info["n_t2"] = pl.n_t2
+    info["plan"] = pl.info
+    cur = c.parity
+    e = float(c.e_last)
+    t1_out = b["t1"][cur].reshape(pl.p, pl.h).clone()
+    dcode = b["state"].dtype
+    if t2_format == "compact":
+        t2_out = b["t2"][cur][:pl.n_t2].clone()
+    else:
+        t2_out = torch.zeros((pl.p, pl.p, pl.h, pl.h), dtype=torch.float64, device=dev)
+        _lib.check(L.nlb_struct_unpack_t2(eng.prob, b["t2"][cur].data_ptr(), dcode, t2_out.data_ptr(), sp),
+                   "unpack")
+    return e, t1_out, t2_out

@@ -295,6 +295,8 @@ CASES = {
     "he4_L4_c2": lambda: case_system("he4_L4_c2", 4, "he4", -6.0, 2.0, store_t2=False),
     "a28_L4": lambda: case_system("a28_L4", 4, "a28", -6.0, 2.0, tight=False, store_t2=False,
                                   traj_steps=2),
+    "a28_L4_tight": lambda: case_system("a28_L4_tight", 4, "a28", -6.0, 2.0, store_t2=False,
+                                        traj_steps=1, eps=1e-13),
     "soa_diis": case_soa_diis,
 }
 

@@ -1,0 +1,139 @@
+"""Structured CUDA engine vs the reference (golden vectors) and the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import golden_io as G
+from nulattice_b200 import ccsd_solver
+from nulattice_b200 import hamiltonian as ham
+from oracle import ccsd_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def _solve(tag, **kw):
+    g = G.load(tag)
+    fock, two = G.hamiltonian(g)
+    info = {}
+    out = ccsd_solver(fock, two, device=DEV, info=info, **kw)
+    assert info["engine"] == "structured", info
+    return g, out, info
+
+
+@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he4_L4_c2"])
+def test_tight_energy_matches_reference(tag):
+    """Fixed point of the reference's own NumPy solver, 1e-10 relative."""
+    g, (e, t1, t2), info = _solve(tag, eps=float(g_eps(tag)), maxSteps=5000, max_diis=0,
+                                  criterion="numpy")
+    ref = float(g["tight_e"])
+    assert info["status"] == "converged"
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
+    np.testing.assert_allclose(t1, g["tight_t1"], atol=1e-10)
+    assert np.linalg.norm(t2) == pytest.approx(float(g["tight_t2_norm"]), rel=1e-9)
+
+
+def g_eps(tag):
+    return float(G.load(tag)["tight_eps"])
+
+
+@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he4_L4_c2"])
+def test_trajectory_matches_reference(tag):
+    g = G.load(tag)
+    _, (e, t1, t2), info = _solve(tag, eps=0.0, maxSteps=int(g["traj_steps"]), max_diis=0,
+                                  criterion="numpy")
+    assert e == pytest.approx(float(g["traj_e"]), rel=1e-12)
+    np.testing.assert_allclose(t1, g["traj_t1"], atol=1e-13)
+    if "traj_t2_idx" in g:
+        np.testing.assert_allclose(t2, G.dense(g, "traj_t2"), atol=1e-13)
+    assert np.linalg.norm(t2) == pytest.approx(float(g["traj_t2_norm"]), rel=1e-11)
+
+
+def test_unmixed_ten_steps():
+    g = G.load("o16_L2")
+    _, (e, t1, _), _ = _solve("o16_L2", eps=0.0, maxSteps=10, max_diis=0, mixing=0.0, criterion="numpy")
+    assert e == pytest.approx(float(g["m0_e"]), rel=1e-12)
+    np.testing.assert_allclose(t1, g["m0_t1"], atol=1e-12)
+
+
+def test_pulsed_diis_matches_torch_solver():
+    d = G.load("soa_diis_he4_L3")
+    for steps in (4, 9, 13):
+        _, (e, t1, t2), _ = _solve("he4_L3_t5", eps=0.0, maxSteps=steps, max_diis=4)
+        assert e == pytest.approx(float(d[f"diis_e_{steps}"]), rel=1e-11)
+        np.testing.assert_allclose(t1, d[f"diis_t1_{steps}"], atol=1e-11)
+        assert np.linalg.norm(t2) == pytest.approx(float(d[f"diis_t2norm_{steps}"]), rel=1e-10)
+
+
+def test_diis_converges_to_reference_fixed_point():
+    g = G.load("he4_L3_t5")
+    _, (e, _, _), info = _solve("he4_L3_t5", eps=1e-13, maxSteps=2000, max_diis=8)
+    assert info["status"] == "converged"
+    assert abs(e - float(g["tight_e"])) <= 1e-10 * abs(float(g["tight_e"]))
+    assert info["iterations"] < int(g["tight_iters"])
+
+
+def test_a28_two_steps_match_reference():
+    g = G.load("a28_L4")
+    e_ref, fock, two = ham.normal_ordered_hamiltonian(4, g["holes"], -6.0, -6.0, 2.0, dense=False)
+    info = {}
+    e, t1, t2 = ccsd_solver(fock, two, eps=0.0, maxSteps=int(g["traj_steps"]), max_diis=0, device=DEV,
+                            criterion="numpy", info=info)
+    assert info["engine"] == "structured"
+    assert e == pytest.approx(float(g["traj_e"]), rel=1e-12)
+    np.testing.assert_allclose(t1, g["traj_t1"], atol=1e-13)
+    assert np.linalg.norm(t2) == pytest.approx(float(g["traj_t2_norm"]), rel=1e-11)
+
+
+@pytest.mark.parametrize("tag", ["he4_L3_c1", "he4_L4_c2"])
+def test_mixed_precision_energy(tag):
+    g = G.load(tag)
+    ref = float(g["tight_e"])
+    _, (e, _, _), info = _solve(tag, eps=1e-12, maxSteps=3000, max_diis=8, precision="mixed",
+                                mixed_eps=1e-7)
+    assert info["status"] == "converged"
+    assert abs(info["mixed_energy"] - ref) <= 1e-6 * abs(ref)
+    assert abs(e - ref) <= 1e-10 * abs(ref)
+
+
+def test_compact_output_and_torch_inputs():
+    g = G.load("he4_L3_c1")
+    fock, two = G.hamiltonian(g)
+    ft = [torch.as_tensor(f, device=DEV) for f in fock]
+    e, t1, t2c = ccsd_solver(ft, two, eps=0.0, maxSteps=3, max_diis=0, device=DEV, criterion="numpy",
+                             t2_format="compact")
+    assert isinstance(t1, torch.Tensor) and t1.device.type == "cuda"
+    from nulattice_b200 import structure as S
+    plan, _ = S.detect(fock, two)
+    np.testing.assert_allclose(plan.unpack_t2(t2c.cpu().numpy()), G.dense(g, "traj_t2"), atol=1e-13)
+
+
+def test_ccs_and_t1initial_match_oracle():
+    g = G.load("he4_L3_c1")
+    fock, two = G.hamiltonian(g)
+    for kw in (dict(ccs=True), dict(t1initial=g["traj_t1"])):
+        e, t1, t2 = ccsd_solver(fock, two, eps=0.0, maxSteps=5, max_diis=0, device=DEV, criterion="numpy", **kw)
+        eo, t1o, t2o, _, _ = O.solve(fock, two, eps=0.0, maxSteps=5, max_diis=0, criterion="numpy", **kw)
+        assert e == pytest.approx(eo, rel=1e-12)
+        np.testing.assert_allclose(t1, t1o, atol=1e-13)
+        np.testing.assert_allclose(t2, t2o, atol=1e-13)
+
+
+def test_max_iter_status():
+    info = {}
+    g = G.load("he4_L3_c1")
+    fock, two = G.hamiltonian(g)
+    ccsd_solver(fock, two, eps=1e-15, maxSteps=7, max_diis=0, device=DEV, info=info)
+    assert info["status"] == "max_iter" and info["iterations"] == 7
+
+
+def test_nan_input_reports_divergence():
+    """A NaN injected on the host into f_pp ends the solve with status diverged."""
+    g = G.load("he4_L3_c1")
+    fock, two = G.hamiltonian(g)
+    fock = [f.copy() for f in fock]
+    fock[0][5, 5] = np.nan
+    info = {}
+    ccsd_solver(fock, two, eps=1e-12, maxSteps=50, max_diis=0, device=DEV, info=info)
+    assert info["status"] == "diverged"

@@ -1,0 +1,124 @@
+"""Host-side logic: Hamiltonian builder, structure detection, channel algebra, C ABI."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import golden_io as G
+import struct_model as M
+from nulattice_b200 import hamiltonian as ham
+from nulattice_b200 import structure as S
+from oracle import ccsd_oracle as O
+
+
+def _canon(rows):
+    d = {}
+    for r in np.asarray(rows).reshape(-1, 5):
+        k = tuple(int(x) for x in r[:4])
+        d[k] = d.get(k, 0.0) + r[4]
+    return {k: v for k, v in d.items() if v != 0}
+
+
+@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he3_L3", "li6x_L3", "he4_L4_c2"])
+def test_builder_matches_reference(tag):
+    g = G.load(tag)
+    vs1 = float(g["vs1"]) if "vs1" in g else float(g["v2"])
+    e, f, two = ham.normal_ordered_hamiltonian(int(g["L"]), g["holes"], float(g["v2"]), vs1, float(g["w3"]))
+    fr, tr = G.hamiltonian(g)
+    assert e == pytest.approx(float(g["e_ref"]), abs=1e-12)
+    for a, b in zip(f, fr):
+        np.testing.assert_allclose(a, b, atol=1e-13)
+    for a, b in zip(two[2:], tr[2:]):
+        np.testing.assert_allclose(a, b, atol=1e-13)
+    assert _canon(two[0]) == pytest.approx(_canon(tr[0]))
+    assert _canon(two[1]) == pytest.approx(_canon(tr[1]))
+
+
+def test_builder_sparse_blocks_equal_dense():
+    e1, f1, t1 = ham.normal_ordered_hamiltonian(3, ham.closed_shell_holes(3, 4), -6, -6, 2, dense=True)
+    e2, f2, t2 = ham.normal_ordered_hamiltonian(3, ham.closed_shell_holes(3, 4), -6, -6, 2, dense=False)
+    assert e1 == e2
+    for a, b in zip(t1[2:], t2[2:]):
+        np.testing.assert_array_equal(a, b.to_dense())
+
+
+def test_units_and_holes():
+    assert ham.phys_unit(2.0) == pytest.approx(0.5 * 197.3269804 ** 2 / (938.92 * 4.0))
+    assert ham.contact_couplings(-3.0, 1.0) == (-6.0, 2.0)
+    h = ham.closed_shell_holes(6, 28)
+    assert len(h) == 28 and len({tuple(x[:3]) for x in h}) == 7
+
+
+@pytest.mark.parametrize("tag,expect", [("o16_L2", True), ("he4_L3_c1", True), ("he3_L3", False),
+                                        ("li6x_L3", False)])
+def test_detect(tag, expect):
+    g = G.load(tag)
+    fock, two = G.hamiltonian(g)
+    plan, why = S.detect(fock, two)
+    assert (plan is not None) == expect, why
+
+
+def test_detect_rejects_structureless_random():
+    r = G.load("dgrams_random")
+    plan, why = S.detect([r["f_pp"], r["f_ph"], r["f_hh"]],
+                         [G.rows(r, "v_pppp"), G.rows(r, "v_ppph"), r["v_pphh"], r["v_phph"], r["v_phhh"],
+                          r["v_hhhh"]])
+    assert plan is None and why
+
+
+def test_compact_layout_roundtrip_and_size():
+    g = G.load("he4_L3_c1")
+    fock, two = G.hamiltonian(g)
+    plan, _ = S.detect(fock, two)
+    assert plan.n_t2 == 6 * 26 * 26
+    t2 = plan.unpack_t2(np.random.default_rng(0).standard_normal(plan.n_t2))
+    np.testing.assert_array_equal(t2, -t2.transpose(1, 0, 2, 3))
+    np.testing.assert_array_equal(t2, -t2.transpose(0, 1, 3, 2))
+    np.testing.assert_array_equal(plan.unpack_t2(plan.pack_t2(t2)), t2)
+
+
+def test_a28_config_sizes():
+    e, fock, two = ham.normal_ordered_hamiltonian(4, ham.closed_shell_holes(4, 28), -6, -6, 2, dense=False)
+    plan, why = S.detect(fock, two)
+    assert plan is not None, why
+    assert plan.n_labels == 4 and len(plan.channels) == 6
+    assert plan.n_t2 == 6 * 57 * 57 * 49
+
+
+@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5"])
+def test_channel_model_matches_reference_trajectory(tag):
+    g = G.load(tag)
+    fock, two = G.hamiltonian(g)
+    plan, _ = S.detect(fock, two)
+    H = O.Hamiltonian(fock, two)
+    t1, B = O.t1_init(H), plan.pack_t2(O.t2_init(H))
+    for _ in range(int(g["traj_steps"])):
+        t1, B = M.iterate(plan, fock, t1, B, 0.5)
+    np.testing.assert_allclose(t1, g["traj_t1"], atol=1e-14)
+    np.testing.assert_allclose(plan.unpack_t2(B), G.dense(g, "traj_t2"), atol=1e-14)
+
+
+def test_channel_model_a28_two_steps():
+    g = G.load("a28_L4")
+    e, fock, two = ham.normal_ordered_hamiltonian(4, g["holes"], -6.0, -6.0, 2.0, dense=False)
+    plan, _ = S.detect(fock, two)
+    H_f = [np.asarray(f) for f in fock]
+    t1 = O.t1_init(O.Hamiltonian(fock, [two[0], two[1]] + [b.to_dense() for b in two[2:]]))
+    B = np.zeros(plan.n_t2)
+    for _ in range(int(g["traj_steps"])):
+        t1, B = M.iterate(plan, H_f, t1, B, 0.5)
+    assert float(np.sum(H_f[1] * t1)) == pytest.approx(float(g["traj_e"]), rel=1e-12)
+    np.testing.assert_allclose(t1, g["traj_t1"], atol=1e-13)
+    assert 2.0 * np.linalg.norm(B) == pytest.approx(float(g["traj_t2_norm"]), rel=1e-12)
+
+
+def test_library_exports_declared_symbols():
+    from nulattice_b200 import _lib
+    L = _lib.lib()
+    syms = _lib.exported_symbols()
+    assert len(syms) >= 8
+    for s in syms:
+        assert hasattr(L, s), s
+    assert L.nlb_version() >= 1
+    assert ctypes.sizeof(_lib.Ctrl) == 1064
+    assert ctypes.sizeof(_lib.StructProblem) == 240
