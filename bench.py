@@ -1,0 +1,353 @@
+"""Benchmark: time to E_CCSD for the L=6, A=28 lattice nucleus on one B200.
+
+Workload: periodic cubic lattice L=6 (864 states), A=28 closed shell (site
+(0,0,0) and its six neighbours, four spin-isospin states each; 836 particle
+states), kinetic hopping + on-site SU(4) contact C2=-3 + three-body contact
+C3=+1 in units of hbar^2/(M a^2) (the reference's unit is half of that, so
+vT1=vS1=-6, w3=+2).  The Hamiltonian is built in-process; nothing is read
+from disk.
+
+A *step* is one complete CCSD solve from the MP2 start:
+
+* ``mixed``: T2 in FP32 with FP64 T1 / energy / DIIS (subspace 8), energy
+  test 1e-8, followed by FP64 steps to eps=1e-10 when ``--refine`` is set;
+* ``fp64``: the plain FP64 path with the reference's own algorithm
+  (Jacobi + mixing 0.5, no DIIS, energy test 1e-8).
+
+``value`` is the mixed time-to-solution (device time, CUDA events, inputs
+resident); its energy must lie within 1e-6 relative of the FP64 fixed point
+(a tight FP64 solve, eps=1e-12, run once untimed).  L2 (126 MB) is flushed
+by a 256 MiB write before every timed solve.
+
+``--impl reference`` times the CPU oracle (a numpy restatement of the
+reference's CCSD, evaluating every diagram as the reference does) on the host
+cores: one Jacobi iteration at L=4, A=28 per step, projected to L=6 by the
+p^3 growth of the dominant dense contractions and multiplied by the FP64
+iteration count at L=6.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-E_CCSD (<=1e-6 rel vs FP64 oracle) and s/iter, mixed vs FP64, 1 B200"
+L_BENCH, A_BENCH, C2, C3 = 6, 28, -3.0, 1.0
+L_SAMPLE = 4                 # CPU sample size (same A=28 closed shell)
+FP64_ITERS_L6 = None         # filled from the FP64 run of the same process
+# FP64 Jacobi iteration count at L=6, A=28 (eps=1e-8), measured by the FP64
+# GPU path; the reference arm runs on the host alone and uses this value.
+FP64_ITERS_L6_MEASURED = 115
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--refine", action="store_true", help="finish the mixed solve with FP64 steps")
+    ap.add_argument("--profile", action="store_true", help="one short mixed solve, no JSON (for ncu)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, ws, local
+
+
+def build_problem(L, A, dense=False):
+    from nulattice_b200 import hamiltonian as ham
+    v2, w3 = ham.contact_couplings(C2, C3)
+    e_ref, fock, two = ham.normal_ordered_hamiltonian(L, ham.closed_shell_holes(L, A), v2, v2, w3, dense=dense)
+    return e_ref, fock, two
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_sample(threads):
+    """One oracle Jacobi iteration at L=4, A=28 (every diagram evaluated)."""
+    import numpy as np
+    from oracle import ccsd_oracle as O
+    O.SKIP_ZERO_BLOCKS = False
+    e_ref, fock, two = build_problem(L_SAMPLE, A_BENCH, dense=True)
+    H = O.Hamiltonian(fock, two)
+    t1, t2 = O.t1_init(H), O.t2_init(H)
+    t0 = time.perf_counter()
+    r = O.ppph_intermediates(H.ppph_idx, H.ppph_val, t1, t2)
+    n1 = O.t1_step(H, t1, t2, r)
+    n2 = O.t2_step(H, t1, t2, r)
+    dt = time.perf_counter() - t0
+    assert np.isfinite(n1).all() and np.isfinite(n2).all()
+    return dt, H.p
+
+
+def projected_tts(s_iter_sample, p_sample, p_bench, iters):
+    return s_iter_sample * (p_bench / p_sample) ** 3 * iters
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np  # noqa: F401
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    p6 = 4 * L_BENCH ** 3 - A_BENCH
+    times = []
+    for k in range(args.warmup + args.steps):
+        dt, p4 = cpu_sample(threads)
+        if k >= args.warmup:
+            times.append(dt)
+    s_iter = statistics.median(times)
+    val = projected_tts(s_iter, p4, p6, FP64_ITERS_L6_MEASURED)
+    sample = (f"one Jacobi iteration of the numpy port of the reference CCSD (every diagram) at "
+              f"L={L_SAMPLE}, A={A_BENCH} (p={p4}), median of {args.steps}: {s_iter:.2f} s; projected to "
+              f"L=6 (p={p6}) by (p6/p4)^3 and x{FP64_ITERS_L6_MEASURED} iterations")
+    out = {"metric": METRIC, "value": val, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": s_iter * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+           "data": "synthetic lattice Hamiltonian built in-process",
+           "config": {"workload": "ccsd_L6_A28", "L": L_BENCH, "A": A_BENCH, "C2": C2, "C3": C3},
+           "cpu_baseline": {"value": val, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+    from nulattice_b200 import _lib
+    from nulattice_b200 import ccsd as C
+    from nulattice_b200 import structure as S
+
+    rank, ws, local = dist_setup()
+    dev = torch.device("cuda", local)
+    e_ref, fock, two = build_problem(L_BENCH, A_BENCH)
+    plan, why = S.detect(fock, two)
+    assert plan is not None, why
+    eng = C.StructuredEngine(plan, fock, dev)
+
+    def solve(precision, t2_events=None, **kw):
+        info = {}
+        if precision == "mixed":
+            e, t1, t2 = C.solve_structured(eng, eps=1e-10 if args.refine else 1e-8, maxSteps=4000, max_diis=8,
+                                           precision="mixed", mixed_eps=1e-8, t2_format="compact",
+                                           info=info, t2_events=t2_events, refine=args.refine, **kw)
+            if not args.refine:
+                info["refine_iters"] = 0
+        else:
+            e, t1, t2 = C.solve_structured(eng, eps=1e-8, maxSteps=4000, max_diis=0, precision="fp64",
+                                           criterion="numpy", t2_format="compact", info=info,
+                                           t2_events=t2_events, **kw)
+        return e, info
+
+    if args.profile:
+        C.solve_structured(eng, eps=0.0, maxSteps=12, max_diis=8, precision="mixed", mixed_eps=0.0,
+                           t2_format="compact")
+        torch.cuda.synchronize()
+        print("profile run done", flush=True)
+        return
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # FP64 fixed point used as the accuracy reference (untimed)
+    e_tight, _, _ = C.solve_structured(eng, eps=1e-12, maxSteps=6000, max_diis=8, precision="fp64",
+                                       t2_format="compact")
+    for _ in range(args.warmup):
+        solve("mixed")
+        solve("fp64")
+    torch.cuda.synchronize()
+
+    def timed(precision):
+        evs, t2ev, infos, energies = [], [], [], []
+        eng.launches = 0
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            e, info = solve(precision, t2_events=t2ev)
+            b.record()
+            evs.append((a, b))
+            infos.append(info)
+            energies.append(e)
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        step_ms = [a.elapsed_time(b) for a, b in evs]
+        k_ms = [a.elapsed_time(b) for a, b in t2ev]
+        return step_ms, k_ms, infos, energies, eng.launches
+
+    dev_index = torch.cuda.current_device()
+    with Clocks(dev_index) as clk:
+        m_ms, m_k, m_info, m_e, m_launch = timed("mixed")
+    clocks = clk.summary()
+    d_ms, d_k, d_info, d_e, _ = timed("fp64")
+
+    def gmax(x):
+        if ws > 1:
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    tts_mixed = gmax(statistics.mean(m_ms)) / 1e3
+    tts_fp64 = gmax(statistics.mean(d_ms)) / 1e3
+    it_mixed = m_info[-1]["iterations"]
+    it_fp64 = d_info[-1]["iterations"]
+    e_corr = m_e[-1]
+    rel = abs((e_corr + e_ref) - (e_tight + e_ref)) / abs(e_tight + e_ref)
+
+    # roofline of the T2 update kernel (mixed, FP32 storage, DIIS ring write)
+    n_t2 = plan.n_t2
+    alg_bytes = (3 * n_t2 + eng.n_g) * 4
+    k_ms = statistics.mean(m_k)
+    achieved = alg_bytes / (k_ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "t2_update_traffic.json")
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get("bytes_per_launch")
+    roofline = {"kernel": "k_t2_update<float>", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "alg_bytes_per_launch": alg_bytes, "avg_launch_us": k_ms * 1e3, "launches": len(m_k)}
+
+    out = {"metric": METRIC, "value": tts_mixed, "unit": "s", "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": tts_mixed * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+           "data": "synthetic: lattice Hamiltonian built in-process (no dataset)",
+           "config": {"workload": "ccsd_L6_A28_mixed", "L": L_BENCH, "A": A_BENCH, "p": plan.p, "h": plan.h,
+                      "C2": C2, "C3": C3, "units": "hbar^2/(M a^2)", "n_t2_compact": n_t2,
+                      "max_diis": 8, "mixed_eps": 1e-8, "refine": bool(args.refine),
+                      "l2": "256 MiB flush write before every timed solve (excluded from step time)",
+                      "parallelism": "replicas" if ws > 1 else "single"},
+           "s_per_iter": tts_mixed / it_mixed, "iterations": it_mixed,
+           "refine_iters": m_info[-1].get("refine_iters", 0),
+           "fp64": {"time_to_solution_s": tts_fp64, "s_per_iter": tts_fp64 / it_fp64, "iterations": it_fp64,
+                    "algorithm": "Jacobi + mixing 0.5, no DIIS (reference NumPy algorithm), eps 1e-8"},
+           "speedup_mixed_vs_fp64": tts_fp64 / tts_mixed,
+           "e_ccsd_mev": (e_corr + e_ref), "e_ccsd_fp64_fixed_point": e_tight + e_ref,
+           "e_ccsd_rel_err": rel, "roofline": roofline, "gpu_launches": m_launch, "clocks": clocks}
+
+    if not args.no_e2e:
+        out["e2e"] = e2e_leg(args, fock, two, dev)
+    if not args.no_cpu and rank == 0:
+        dt, p4 = cpu_sample(os.cpu_count())
+        val = projected_tts(dt, p4, plan.p, it_fp64)
+        out["cpu_baseline"] = {"value": val, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"one Jacobi iteration of the numpy port (every diagram) at L={L_SAMPLE}, "
+                                         f"A={A_BENCH} (p={p4}): {dt:.2f} s, projected to p={plan.p} by "
+                                         f"(p/p4)^3 and x{it_fp64} FP64 iterations"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def e2e_leg(args, fock, two, dev):
+    """The public ccsd_solver on host (numpy) inputs: H2D of the Hamiltonian,
+    plan build, mixed solve, D2H of E, t1 and the compact t2."""
+    import numpy as np
+    import torch
+    from nulattice_b200 import ccsd_solver
+    h2d = sum(np.asarray(f).nbytes for f in fock) + sum(
+        (b.indices.nbytes + b.values.nbytes) if hasattr(b, "indices") else np.asarray(b).nbytes for b in two)
+    times = []
+    for k in range(args.warmup + args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        info = {}
+        e, t1, t2 = ccsd_solver(fock, two, eps=1e-8, maxSteps=4000, max_diis=8, device=dev, precision="mixed",
+                                mixed_eps=1e-8, t2_format="compact", info=info)
+        b.record()
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            times.append(a.elapsed_time(b) / 1e3)
+    d2h = 8 + t1.nbytes + t2.nbytes
+    return {"value": statistics.mean(times), "unit": "s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "iterations": info.get("iterations")}
+
+
+if __name__ == "__main__":
+    main()

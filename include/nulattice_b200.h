@@ -33,14 +33,17 @@ enum { NLB_OK = 0, NLB_ERR_ARG = 1, NLB_ERR_LAUNCH = 2, NLB_ERR_SIZE = 3, NLB_ER
 enum { NLB_F64 = 0, NLB_F32 = 1 };
 enum { NLB_RUNNING = 0, NLB_CONVERGED = 1, NLB_MAX_ITER = 2, NLB_DIVERGED = 3 };
 enum { NLB_CRIT_SOA = 0, NLB_CRIT_NUMPY = 1 };
+enum { NLB_STAGE_PREP = 0, NLB_STAGE_GTERMS = 1, NLB_STAGE_T2 = 2, NLB_STAGE_T1 = 3, NLB_STAGE_FINISH = 4 };
 
 /* One channel (label pair g1 < g2) of the compact T2: a dense block
- * B[a'][b'][i'][j'] of np1*np2*nh1*nh2 numbers at element `offset`. */
+ * B[a'][b'][i'][j'] of np1*np2*nh1*nh2 numbers at element `offset`.  A "row"
+ * is B[a'][:][:] (np2*nh1*nh2 numbers). */
 typedef struct {
     int32_t g1, g2, np1, np2, nh1, nh2;
     int32_t pb1, pb2, hb1, hb2;   /* label bases into p_ord / h_ord */
     int64_t offset;               /* element offset in compact T2 */
-    int64_t gb_off, ga_off;       /* element offsets of the G intermediates */
+    int64_t ga_off;               /* offset of Ga[k'][b'][i'j'] (nh1*np2*nh1*nh2) */
+    int64_t f2_off;               /* offset of the T1 Fock term F2[a'][i'] (np1*nh1) */
     int64_t hh_ptr_off, hh_col_off, pp_ptr_off, pp_col_off;
 } nlb_channel;
 
@@ -49,10 +52,20 @@ typedef struct {
 typedef struct {
     int32_t p, h, n_labels, n_channels;
     int64_t n_t2;                 /* compact T2 length */
-    int64_t n_g;                  /* G-intermediate length */
+    int64_t n_g;                  /* Ga length (sum over channels) */
+    int64_t n_f2;                 /* F2 length (sum of np1*nh1) */
+    int64_t n_rows;               /* sum of np1: one T2-update task per row */
+    int64_t n_t1c, n_xc;          /* compact T1 / X_hh table lengths */
+    int32_t max_row;              /* max np2*nh1*nh2 */
+    int32_t max_nh;               /* max holes in one label */
+    int32_t uniform_nh;           /* every channel has nh1 == nh2 == this (0: not uniform) */
+    int32_t diag_ladders;         /* 1: both ladders only couple a pair to itself */
     const nlb_channel *chan;      /* [n_channels] */
     const int64_t *t2_end;        /* [n_channels] cumulative end of each block */
-    const int64_t *g_end;         /* [n_channels] cumulative end of G items */
+    const int64_t *g_end;         /* [n_channels] cumulative end of Ga blocks */
+    const int64_t *row_end;       /* [n_channels] cumulative row count */
+    const int32_t *t1c_base;      /* [n_labels+1] offsets of t1[P_g, H_g] tables */
+    const int32_t *xc_base;       /* [n_labels+1] offsets of X_hh[H_g, H_g] tables */
     const int32_t *p_ord;         /* [p] particle index of label-ordered row */
     const int32_t *h_ord;         /* [h] */
     const int32_t *p_label, *h_label, *p_loc, *h_loc;   /* [p], [h], [p], [h] */
@@ -92,8 +105,9 @@ typedef struct {
 typedef struct {
     double *t1[2];      /* [p*h] double-buffered T1 */
     void *t2[2];        /* [n_t2] double-buffered compact T2 (dtype) */
-    void *g;            /* [n_g] G intermediates (dtype) */
-    double *prep;       /* [nlb_struct_prep_len(p,h)] dressed-Fock scratch */
+    void *g;            /* [n_g] Ga intermediates (dtype) */
+    void *f2;           /* [n_f2] T1 Fock-term partial sums (dtype) */
+    double *prep;       /* [nlb_struct_prep_len(prob)] dressed-Fock scratch */
     double *diis_t1;    /* [max_diis * p*h] T1 error ring (may be NULL) */
     void *diis_t2;      /* [max_diis * n_t2] T2 error ring (dtype, may be NULL) */
     nlb_ctrl *ctrl;
@@ -105,8 +119,13 @@ int nlb_version(void);
 const char *nlb_last_error(void);
 
 /* Length (doubles) of the dressed-Fock scratch: Q, X_hh (T2 eq), X_hh (T1 eq)
- * as h*h each, and the particle diagonals of X_pp for both equations. */
-int64_t nlb_struct_prep_len(int32_t p, int32_t h);
+ * as h*h each, the particle diagonals of X_pp for both equations, and the
+ * per-label compact tables t1[P_g,H_g], X_hh[H_g,H_g], diag X_pp, diag X_hh. */
+int64_t nlb_struct_prep_len(const nlb_struct_problem *prob);
+
+/* Dynamic shared memory (bytes) the T2-update kernel needs per block for
+ * this problem and dtype; 0 when it exceeds the device limit. */
+int64_t nlb_struct_smem_bytes(const nlb_struct_problem *prob, int32_t dtype);
 
 /* Reset `ctrl` on the device and load the solver parameters. */
 int nlb_struct_ctrl_init(nlb_ctrl *ctrl, double eps, double mixing, int32_t max_steps,
@@ -123,11 +142,18 @@ int nlb_struct_ctrl_init(nlb_ctrl *ctrl, double eps, double mixing, int32_t max_
 int nlb_struct_step(const nlb_struct_problem *prob, const nlb_struct_state *st,
                     nlb_stream_t stream);
 
+/* The five launches of nlb_struct_step one at a time (NLB_STAGE_*), so a
+ * caller can bracket a single kernel with events.  Running the stages
+ * PREP..FINISH in order is exactly one nlb_struct_step. */
+int nlb_struct_stage(const nlb_struct_problem *prob, const nlb_struct_state *st, int32_t stage,
+                     nlb_stream_t stream);
+
 /* Pulsed DIIS of the torch solver (CCM/soa/coupled_cluster.py:522-567): when
  * ctrl->diis_pulse is set, build the Gram matrix of the stored error vectors
  * (FP64), solve the bordered system in FP64 on the device and extrapolate the
- * current amplitudes in place.  No-op otherwise. */
-int nlb_struct_diis(const nlb_struct_problem *prob, const nlb_struct_state *st,
+ * current amplitudes in place.  No-op otherwise.  `max_diis` must equal the
+ * value given to nlb_struct_ctrl_init (it selects the compiled kernel). */
+int nlb_struct_diis(const nlb_struct_problem *prob, const nlb_struct_state *st, int32_t max_diis,
                     nlb_stream_t stream);
 
 /* Energy of the current amplitudes, sum_ai f_ai t1_ai (ccsd_energy,

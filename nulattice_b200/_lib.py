@@ -18,6 +18,7 @@ NLB_OK, NLB_ERR_ARG, NLB_ERR_LAUNCH, NLB_ERR_SIZE, NLB_ERR_CUDA = 0, 1, 2, 3, 4
 NLB_F64, NLB_F32 = 0, 1
 NLB_RUNNING, NLB_CONVERGED, NLB_MAX_ITER, NLB_DIVERGED = 0, 1, 2, 3
 NLB_CRIT_SOA, NLB_CRIT_NUMPY = 0, 1
+NLB_STAGE_PREP, NLB_STAGE_GTERMS, NLB_STAGE_T2, NLB_STAGE_T1, NLB_STAGE_FINISH = 0, 1, 2, 3, 4
 MAX_DIIS = 10
 
 c_int32, c_int64, c_double, c_void_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
@@ -25,15 +26,17 @@ c_int32, c_int64, c_double, c_void_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_
 # numpy mirror of nlb_channel (device array of channel descriptors)
 CHANNEL_DTYPE = np.dtype([(n, np.int32) for n in ("g1", "g2", "np1", "np2", "nh1", "nh2",
                                                   "pb1", "pb2", "hb1", "hb2")] +
-                         [(n, np.int64) for n in ("offset", "gb_off", "ga_off", "hh_ptr_off",
+                         [(n, np.int64) for n in ("offset", "ga_off", "f2_off", "hh_ptr_off",
                                                   "hh_col_off", "pp_ptr_off", "pp_col_off")])
 assert CHANNEL_DTYPE.itemsize == 96
 
 
 class StructProblem(ctypes.Structure):
-    _fields_ = [("p", c_int32), ("h", c_int32), ("n_labels", c_int32), ("n_channels", c_int32),
-                ("n_t2", c_int64), ("n_g", c_int64)] + [
-        (n, c_void_p) for n in ("chan", "t2_end", "g_end", "p_ord", "h_ord", "p_label", "h_label",
+    _fields_ = [("p", c_int32), ("h", c_int32), ("n_labels", c_int32), ("n_channels", c_int32)] + \
+               [(n, c_int64) for n in ("n_t2", "n_g", "n_f2", "n_rows", "n_t1c", "n_xc")] + \
+               [("max_row", c_int32), ("max_nh", c_int32), ("uniform_nh", c_int32), ("diag_ladders", c_int32)] + [
+        (n, c_void_p) for n in ("chan", "t2_end", "g_end", "row_end", "t1c_base", "xc_base",
+                                "p_ord", "h_ord", "p_label", "h_label",
                                 "p_loc", "h_loc", "p_base", "h_base", "fpp_ptr", "fpp_col", "fpp_val",
                                 "fpp_diag", "fph_ptr", "fph_col", "fph_val", "f_ph", "f_hh",
                                 "hh_ptr", "hh_col", "hh_val", "pp_ptr", "pp_col", "pp_val")]
@@ -47,7 +50,8 @@ class Ctrl(ctypes.Structure):
 
 
 class StructState(ctypes.Structure):
-    _fields_ = [("t1", c_void_p * 2), ("t2", c_void_p * 2), ("g", c_void_p), ("prep", c_void_p),
+    _fields_ = [("t1", c_void_p * 2), ("t2", c_void_p * 2), ("g", c_void_p), ("f2", c_void_p),
+                ("prep", c_void_p),
                 ("diis_t1", c_void_p), ("diis_t2", c_void_p), ("ctrl", c_void_p), ("dtype", c_int32)]
 
 
@@ -71,11 +75,17 @@ def lib():
     L.nlb_version.restype = c_int32
     L.nlb_last_error.restype = ctypes.c_char_p
     L.nlb_struct_prep_len.restype = c_int64
-    L.nlb_struct_prep_len.argtypes = [c_int32, c_int32]
+    L.nlb_struct_prep_len.argtypes = [ctypes.POINTER(StructProblem)]
+    L.nlb_struct_smem_bytes.restype = c_int64
+    L.nlb_struct_smem_bytes.argtypes = [ctypes.POINTER(StructProblem), c_int32]
     L.nlb_struct_ctrl_init.argtypes = [c_void_p, c_double, c_double, c_int32, c_int32, c_int32, c_int32,
                                        c_double, c_void_p]
-    for name in ("nlb_struct_step", "nlb_struct_diis"):
-        getattr(L, name).argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_void_p]
+    L.nlb_struct_step.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_void_p]
+    L.nlb_struct_diis.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_int32,
+                                  c_void_p]
+    L.nlb_struct_stage.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_int32,
+                                   c_void_p]
+    L.nlb_struct_stage.restype = c_int32
     L.nlb_struct_energy.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_void_p,
                                     c_void_p]
     L.nlb_convert.argtypes = [c_void_p, c_int32, c_void_p, c_int32, c_int64, c_void_p]

@@ -94,28 +94,39 @@ class StructuredEngine:
         p_ord = np.concatenate([pl.p_of[g] for g in range(G)]).astype(np.int32)
         h_ord = np.concatenate([pl.h_of[g] for g in range(G)]).astype(np.int32)
         chans = np.zeros(max(len(pl.channels), 1), dtype=_lib.CHANNEL_DTYPE)
-        t2_end, g_end = [], []
+        t2_end, g_end, row_end = [], [], []
         hh_ptr, hh_col, hh_val, pp_ptr, pp_col, pp_val = [], [], [], [], [], []
-        goff = hp_off = hc_off = pp_off = pc_off = 0
+        goff = foff = rows = hp_off = hc_off = pp_off = pc_off = 0
+        max_row = 1
         for n, ch in enumerate(pl.channels):
             nhp = ch.nh1 * ch.nh2
-            n_gb = ch.np1 * ch.nh2 * nhp
-            n_ga = ch.np2 * ch.nh1 * nhp
+            n_ga = ch.nh1 * ch.np2 * nhp
             chans[n] = (ch.g1, ch.g2, ch.np1, ch.np2, ch.nh1, ch.nh2,
                         pl.p_base[ch.g1], pl.p_base[ch.g2], pl.h_base[ch.g1], pl.h_base[ch.g2],
-                        ch.offset, goff, goff + n_gb, hp_off, hc_off, pp_off, pc_off)
-            goff += n_gb + n_ga
+                        ch.offset, goff, foff, hp_off, hc_off, pp_off, pc_off)
+            goff += n_ga
+            foff += ch.np1 * ch.nh1
+            rows += ch.np1
+            max_row = max(max_row, ch.np2 * nhp)
             t2_end.append(ch.offset + ch.size)
             g_end.append(goff)
+            row_end.append(rows)
             hh_ptr.append(pl.hh_ptr[n]); hh_col.append(pl.hh_col[n]); hh_val.append(pl.hh_val[n])
             pp_ptr.append(pl.pp_ptr[n]); pp_col.append(pl.pp_col[n]); pp_val.append(pl.pp_val[n])
             hp_off += len(pl.hh_ptr[n]); hc_off += len(pl.hh_col[n])
             pp_off += len(pl.pp_ptr[n]); pc_off += len(pl.pp_col[n])
+        n_p = np.array([len(x) for x in pl.p_of]); n_h = np.array([len(x) for x in pl.h_of])
+        t1c_base = np.concatenate([[0], np.cumsum(n_p * n_h)]).astype(np.int32)
+        xc_base = np.concatenate([[0], np.cumsum(n_h * n_h)]).astype(np.int32)
+        self.n_f2, self.n_rows, self.max_row = foff, rows, max_row
+        self.max_nh = int(max(1, n_h.max() if len(n_h) else 1))
+        self.n_t1c, self.n_xc = int(t1c_base[-1]), int(xc_base[-1])
         self.n_g = goff
         cat = lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(1, dt)  # noqa: E731
         T = {}
         T["chan"] = torch.as_tensor(chans.view(np.uint8), device=dev)
-        T["t2_end"] = i64(t2_end or [0]); T["g_end"] = i64(g_end or [0])
+        T["t2_end"] = i64(t2_end or [0]); T["g_end"] = i64(g_end or [0]); T["row_end"] = i64(row_end or [0])
+        T["t1c_base"] = i32(t1c_base); T["xc_base"] = i32(xc_base)
         T["p_ord"] = i32(p_ord); T["h_ord"] = i32(h_ord)
         T["p_label"] = i32(pl.p_label); T["h_label"] = i32(pl.h_label)
         T["p_loc"] = i32(pl.p_loc); T["h_loc"] = i32(pl.h_loc)
@@ -132,11 +143,27 @@ class StructuredEngine:
         self.tables = T
         prob = _lib.StructProblem()
         prob.p, prob.h, prob.n_labels, prob.n_channels = pl.p, pl.h, G, len(pl.channels)
-        prob.n_t2, prob.n_g = pl.n_t2, self.n_g
+        prob.n_t2, prob.n_g, prob.n_f2, prob.n_rows = pl.n_t2, self.n_g, self.n_f2, self.n_rows
+        prob.n_t1c, prob.n_xc, prob.max_row, prob.max_nh = self.n_t1c, self.n_xc, self.max_row, self.max_nh
+        nhs = {(ch.nh1, ch.nh2) for ch in pl.channels}
+        uniform = 0
+        if len(nhs) == 1:
+            n1, n2 = next(iter(nhs))
+            uniform = n1 if n1 == n2 else 0
+        prob.uniform_nh = uniform
+        diag = True
+        for n, ch in enumerate(pl.channels):
+            for ptr, col in ((pl.hh_ptr[n], pl.hh_col[n]), (pl.pp_ptr[n], pl.pp_col[n])):
+                cnt = np.diff(ptr)
+                rows_ = np.repeat(np.arange(len(cnt)), cnt)
+                if np.any(cnt > 1) or np.any(col != rows_):
+                    diag = False
+        prob.diag_ladders = int(diag)
         for k, v in T.items():
             setattr(prob, k, v.data_ptr())
         self.prob = prob
         self._bufs = {}
+        self.launches = 0
 
     # -- buffers ---------------------------------------------------------
     def buffers(self, dtype_code, max_diis):
@@ -150,7 +177,8 @@ class StructuredEngine:
             t1=[torch.zeros(pl.p * pl.h, dtype=torch.float64, device=dev) for _ in range(2)],
             t2=[torch.zeros(max(pl.n_t2, 1), dtype=tdt, device=dev) for _ in range(2)],
             g=torch.zeros(max(self.n_g, 1), dtype=tdt, device=dev),
-            prep=torch.zeros(int(L.nlb_struct_prep_len(pl.p, pl.h)), dtype=torch.float64, device=dev),
+            f2=torch.zeros(max(self.n_f2, 1), dtype=tdt, device=dev),
+            prep=torch.zeros(int(L.nlb_struct_prep_len(self.prob)), dtype=torch.float64, device=dev),
             ctrl=torch.zeros(ctypes_sizeof_ctrl(), dtype=torch.uint8, device=dev),
             diis_t1=torch.zeros(max(max_diis, 1) * pl.p * pl.h, dtype=torch.float64, device=dev)
             if max_diis else None,
@@ -160,7 +188,8 @@ class StructuredEngine:
         st = _lib.StructState()
         st.t1[0], st.t1[1] = b["t1"][0].data_ptr(), b["t1"][1].data_ptr()
         st.t2[0], st.t2[1] = b["t2"][0].data_ptr(), b["t2"][1].data_ptr()
-        st.g, st.prep, st.ctrl = b["g"].data_ptr(), b["prep"].data_ptr(), b["ctrl"].data_ptr()
+        st.g, st.f2 = b["g"].data_ptr(), b["f2"].data_ptr()
+        st.prep, st.ctrl = b["prep"].data_ptr(), b["ctrl"].data_ptr()
         st.diis_t1 = b["diis_t1"].data_ptr() if max_diis else None
         st.diis_t2 = b["diis_t2"].data_ptr() if max_diis else None
         st.dtype = dtype_code
@@ -168,13 +197,39 @@ class StructuredEngine:
         self._bufs[key] = b
         return b
 
+    def _graph_for(self, b, chunk, max_diis, issue):
+        """CUDA graph of `chunk` steps (+ the DIIS pulse) on buffers `b`.
+
+        Every kernel reads its buffer parity and status from the device, so
+        the same graph serves every chunk of every solve on these buffers."""
+        key = ("graph", chunk, max_diis)
+        if key in b:
+            return b[key]
+        dev = self.dev
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            # the kernels are run once outside capture by the caller's first
+            # chunk; here they are only recorded
+            with torch.cuda.graph(g, stream=side):
+                issue_on = _issue_factory(self, b, max_diis, side)
+                issue_on(chunk)
+        torch.cuda.current_stream(dev).wait_stream(side)
+        b[key] = g
+        return g
+
     def read_ctrl(self, b):
         raw = b["ctrl"].cpu().numpy().tobytes()
         return _lib.Ctrl.from_buffer_copy(raw)
 
     # -- one phase of iterations ------------------------------------------
     def run(self, b, t1_init, t2c_init, e0, eps, mixing, max_steps, criterion, max_diis, ccs,
-            verbose=False, sync_every=16, step_offset=0):
+            verbose=False, sync_every=16, step_offset=0, t2_events=None, graph=True):
+        """Iterate until the device-side test stops the solve.
+
+        ``t2_events``: a list to receive one (start, end) CUDA-event pair per
+        T2-update launch (the stages are then launched one by one)."""
         L = _lib.lib()
         dev = self.dev
         stream = torch.cuda.current_stream(dev)
@@ -186,19 +241,49 @@ class StructuredEngine:
             b["t2"][0].copy_(t2c_init)
         b["t2"][1].zero_()
         b["g"].zero_()
+        b["f2"].zero_()
         st = b["state"]
         _lib.check(L.nlb_struct_ctrl_init(b["ctrl"].data_ptr(), eps, mixing, max_steps, criterion,
                                           max_diis, int(bool(ccs)), e0, sp), "ctrl_init")
         use_diis = max_diis > 0 and criterion == _lib.NLB_CRIT_SOA
+        # a chunk of steps ends on a DIIS pulse, so it is periodic
+        chunk = max_diis if use_diis else sync_every
+        if use_diis:
+            while chunk < 8:
+                chunk += max_diis
+        use_graph = graph and not verbose and t2_events is None
+
+        def issue(n_steps, done0):
+            for k in range(n_steps):
+                if t2_events is None:
+                    _lib.check(L.nlb_struct_step(self.prob, st, sp), "step")
+                else:
+                    for stage in range(_lib.NLB_STAGE_PREP, _lib.NLB_STAGE_FINISH + 1):
+                        if stage == _lib.NLB_STAGE_T2:
+                            ev0 = torch.cuda.Event(enable_timing=True)
+                            ev1 = torch.cuda.Event(enable_timing=True)
+                            ev0.record(stream)
+                        _lib.check(L.nlb_struct_stage(self.prob, st, stage, sp), "stage")
+                        if stage == _lib.NLB_STAGE_T2:
+                            ev1.record(stream)
+                            t2_events.append((ev0, ev1))
+                self.launches += 5
+                if use_diis and (done0 + k + 1) % max_diis == 0:
+                    _lib.check(L.nlb_struct_diis(self.prob, st, max_diis, sp), "diis")
+                    self.launches += 4
+
         done = 0
         prev = e0
         while done < max_steps:
-            n = 1 if verbose else min(sync_every, max_steps - done)
-            for _ in range(n):
-                _lib.check(L.nlb_struct_step(self.prob, st, sp), "step")
-                done += 1
-                if use_diis and done % max_diis == 0:
-                    _lib.check(L.nlb_struct_diis(self.prob, st, sp), "diis")
+            n = 1 if verbose else min(chunk, max_steps - done)
+            if use_graph and n == chunk and b.get("warm"):
+                g = self._graph_for(b, chunk, max_diis if use_diis else 0, issue)
+                g.replay()
+                self.launches += (5 * chunk + (4 * (chunk // max_diis) if use_diis else 0))
+            else:
+                issue(n, done)
+                b["warm"] = True
+            done += n
             c = self.read_ctrl(b)
             if verbose:
                 e = c.e_last
@@ -209,6 +294,19 @@ class StructuredEngine:
                 break
         c = self.read_ctrl(b)
         return c
+
+
+def _issue_factory(eng, b, max_diis, stream):
+    L = _lib.lib()
+    sp = ctypes_void(stream.cuda_stream)
+    st = b["state"]
+
+    def issue(n):
+        for k in range(n):
+            _lib.check(L.nlb_struct_step(eng.prob, st, sp), "step")
+            if max_diis and (k + 1) % max_diis == 0:
+                _lib.check(L.nlb_struct_diis(eng.prob, st, max_diis, sp), "diis")
+    return issue
 
 
 def ctypes_sizeof_ctrl():
@@ -288,7 +386,7 @@ def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000
 
 def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5,
                      verbose=False, ccs=False, criterion="soa", precision="fp64", t2_format="dense",
-                     mixed_eps=None, info=None, sync_every=16):
+                     mixed_eps=None, info=None, sync_every=16, t2_events=None, refine=True):
     """Run the structured engine (already built); see :func:`ccsd_solver`."""
     info = {} if info is None else info
     L = _lib.lib()
@@ -307,12 +405,13 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
     if precision == "mixed":
         b32 = eng.buffers(_lib.NLB_F32, diis)
         me = float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)
-        c = eng.run(b32, t1_dev, None, e0, me, mixing, maxSteps, crit, diis, ccs, verbose, sync_every)
+        c = eng.run(b32, t1_dev, None, e0, me, mixing, maxSteps, crit, diis, ccs, verbose, sync_every,
+                    t2_events=t2_events)
         iters += c.iter
         info["mixed_iters"] = c.iter
         info["mixed_energy"] = c.e_last
         status = _STATUS[c.status]
-        if status == "converged" and c.e_last == c.e_last and maxSteps - iters > 0:
+        if refine and status == "converged" and c.e_last == c.e_last and maxSteps - iters > 0:
             # continue in FP64 from the FP32 amplitudes
             b64 = eng.buffers(_lib.NLB_F64, diis)
             cur = c.parity
@@ -320,6 +419,7 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
                                      _lib.NLB_F64, pl.n_t2, sp), "convert")
             c = eng.run(b64, b32["t1"][cur].clone(), b64["t2"][0], c.e_last, eps, mixing, maxSteps - iters,
                         crit, diis, ccs, verbose, sync_every, step_offset=iters)
+            eng.launches += 1
             iters += c.iter
             info["refine_iters"] = c.iter
             b = b64
@@ -327,7 +427,8 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
             b = b32
     else:
         b = eng.buffers(_lib.NLB_F64, diis)
-        c = eng.run(b, t1_dev, None, e0, eps, mixing, maxSteps, crit, diis, ccs, verbose, sync_every)
+        c = eng.run(b, t1_dev, None, e0, eps, mixing, maxSteps, crit, diis, ccs, verbose, sync_every,
+                    t2_events=t2_events)
         iters += c.iter
     torch.cuda.current_stream(dev).synchronize()
     info["t_iterate"] = time.perf_counter() - t0

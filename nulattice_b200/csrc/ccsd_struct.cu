@@ -48,6 +48,7 @@ static int check_launch(const char* where) {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kRowThreads = 256;   // T2 row kernel
 
 __device__ __forceinline__ int find_seg(const int64_t* end, int n, int64_t e) {
     int lo = 0, hi = n - 1;
@@ -78,47 +79,122 @@ __device__ double block_sum(double v) {
 }
 
 // ---------------------------------------------------------------- prep ----
-// Q[k,j] = sum_c f_ck t1_cj; X_hh for the T2 equation (-f_hh - Q) and for the
-// T1 equation (-f_hh - Q/2); diagonals of X_pp: f_aa - S_a and f_aa - S_a/2,
-// S_a = sum_k f_ak t1_ak (coupled_cluster.py:385-399, 501-515).
+// Layout of the scratch (doubles), see nlb_struct_prep_len:
+//   Q[h*h]   Q[k,j] = sum_c f_ck t1_cj
+//   Xh2[h*h] X_hh of the T2 equation, -f_hh - Q      (coupled_cluster.py:505-513)
+//   Xh1[h*h] X_hh of the T1 equation, -f_hh - Q/2    (coupled_cluster.py:388-393)
+//   dXp2[p], dXp1[p]  diagonals of X_pp: f_aa - S_a, f_aa - S_a/2, S_a = sum_k f_ak t1_ak
+//   t1c[n_t1c]  t1[P_g[a'], H_g[k']] per label (a' major)
+//   xc[n_xc]    Xh2[H_g[k'], H_g[i']] per label (k' major)
+//   dpc[p]      dXp2 in label order
+//   dhc[h]      diag Xh2 in label order
+struct PrepView {
+    double *Q, *Xh2, *Xh1, *dXp2, *dXp1, *t1c, *xc, *dpc, *dhc;
+};
+
+__host__ __device__ inline PrepView prep_view(double* base, const nlb_struct_problem& P) {
+    const int64_t hh = (int64_t)P.h * P.h;
+    PrepView v;
+    v.Q = base;
+    v.Xh2 = v.Q + hh;
+    v.Xh1 = v.Xh2 + hh;
+    v.dXp2 = v.Xh1 + hh;
+    v.dXp1 = v.dXp2 + P.p;
+    v.t1c = v.dXp1 + P.p;
+    v.xc = v.t1c + P.n_t1c;
+    v.dpc = v.xc + P.n_xc;
+    v.dhc = v.dpc + P.p;
+    return v;
+}
+
+__device__ __forceinline__ int find_label(const int32_t* base, int G, int64_t u) {
+    int lo = 0, hi = G - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (u >= base[mid]) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Q[k,i] = sum_c f_ck t1_ci using the f_ph column list of hole k.
+__device__ __forceinline__ double q_entry(const nlb_struct_problem& P, const double* t1, int k, int i) {
+    const int g = P.h_label[k];
+    const int row = P.h_base[g] + P.h_loc[k];
+    const int pb = P.p_base[g];
+    double q = 0.0;
+    for (int e = P.fph_ptr[row]; e < P.fph_ptr[row + 1]; ++e)
+        q += P.fph_val[e] * t1[(int64_t)P.p_ord[pb + P.fph_col[e]] * P.h + i];
+    return q;
+}
+
+__device__ __forceinline__ double s_entry(const nlb_struct_problem& P, const double* t1, int a) {
+    double s = 0.0;
+    for (int k = 0; k < P.h; ++k) s += P.f_ph[(int64_t)a * P.h + k] * t1[(int64_t)a * P.h + k];
+    return s;
+}
+
 __global__ void k_prep(nlb_struct_problem P, nlb_struct_state S) {
     const nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
     const double* t1 = S.t1[c->parity];
-    const int h = P.h, p = P.p;
-    double* Q = S.prep;
-    double* Xh2 = Q + (int64_t)h * h;
-    double* Xh1 = Xh2 + (int64_t)h * h;
-    double* dXp2 = Xh1 + (int64_t)h * h;
-    double* dXp1 = dXp2 + p;
-    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid < (int64_t)h * h) {
-        int k = (int)(tid / h), j = (int)(tid % h);
-        int g = P.h_label[k];
-        int row = P.h_base[g] + P.h_loc[k];
-        int pb = P.p_base[g];
-        double q = 0.0;
-        for (int e = P.fph_ptr[row]; e < P.fph_ptr[row + 1]; ++e)
-            q += P.fph_val[e] * t1[(int64_t)P.p_ord[pb + P.fph_col[e]] * h + j];
-        Q[tid] = q;
-        Xh2[tid] = -P.f_hh[tid] - q;
-        Xh1[tid] = -P.f_hh[tid] - 0.5 * q;
-    } else if (tid < (int64_t)h * h + p) {
-        int a = (int)(tid - (int64_t)h * h);
-        double s = 0.0;
-        for (int k = 0; k < h; ++k) s += P.f_ph[(int64_t)a * h + k] * t1[(int64_t)a * h + k];
-        dXp2[a] = P.fpp_diag[a] - s;
-        dXp1[a] = P.fpp_diag[a] - 0.5 * s;
+    const int h = P.h, p = P.p, G = P.n_labels;
+    const PrepView V = prep_view(S.prep, P);
+    int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t hh = (int64_t)h * h;
+    if (u < hh) {
+        const int k = (int)(u / h), j = (int)(u % h);
+        const double q = q_entry(P, t1, k, j);
+        V.Q[u] = q;
+        V.Xh2[u] = -P.f_hh[u] - q;
+        V.Xh1[u] = -P.f_hh[u] - 0.5 * q;
+        return;
+    }
+    u -= hh;
+    if (u < p) {
+        const double s = s_entry(P, t1, (int)u);
+        V.dXp2[u] = P.fpp_diag[u] - s;
+        V.dXp1[u] = P.fpp_diag[u] - 0.5 * s;
+        return;
+    }
+    u -= p;
+    if (u < P.n_t1c) {
+        const int g = find_label(P.t1c_base, G, u);
+        const int nh = P.h_base[g + 1] - P.h_base[g];
+        const int loc = (int)(u - P.t1c_base[g]);
+        const int ap = loc / nh, kq = loc - ap * nh;
+        V.t1c[u] = t1[(int64_t)P.p_ord[P.p_base[g] + ap] * h + P.h_ord[P.h_base[g] + kq]];
+        return;
+    }
+    u -= P.n_t1c;
+    if (u < P.n_xc) {
+        const int g = find_label(P.xc_base, G, u);
+        const int nh = P.h_base[g + 1] - P.h_base[g];
+        const int loc = (int)(u - P.xc_base[g]);
+        const int kq = loc / nh, iq = loc - kq * nh;
+        const int k = P.h_ord[P.h_base[g] + kq], i = P.h_ord[P.h_base[g] + iq];
+        V.xc[u] = -P.f_hh[(int64_t)k * h + i] - q_entry(P, t1, k, i);
+        return;
+    }
+    u -= P.n_xc;
+    if (u < p) {
+        const int a = P.p_ord[u];
+        V.dpc[u] = P.fpp_diag[a] - s_entry(P, t1, a);
+        return;
+    }
+    u -= p;
+    if (u < h) {
+        const int i = P.h_ord[u];
+        V.dhc[u] = -P.f_hh[(int64_t)i * h + i] - q_entry(P, t1, i, i);
     }
 }
 
-// ----------------------------------------------------------- G terms ----
-// Gb[a',k',hp] = sum_c f_ck B[a',c',hp]  (k a hole of label g2)
-// Ga[b',k',hp] = sum_c f_ck B[c',b',hp]  (k a hole of label g1)
-// They carry the rank-h part of X_pp (f_ph t1^T) in the T2 equation and the
-// Fock term f_ck t2_acik of the T1 equation.
+// ---------------------------------------------------------------- Ga ----
+// Ga[k'][b'][i'j'] = sum_c f_ck B[c'][b'][i'j']  (k = hole k' of label g1):
+// the f_ph^T t2 half-contraction along the first particle index.  With t1 it
+// gives the rank-h part of X_pp t2 along a, and it holds the T1 Fock term
+// f_ck t2_acik for particles of label g2.
 template <typename T>
-__global__ void k_gterms(nlb_struct_problem P, nlb_struct_state S) {
+__global__ void k_ga(nlb_struct_problem P, nlb_struct_state S) {
     const nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING || c->ccs) return;
     const T* B = static_cast<const T*>(S.t2[c->parity]);
@@ -127,124 +203,252 @@ __global__ void k_gterms(nlb_struct_problem P, nlb_struct_state S) {
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < P.n_g; e += stride) {
         const int ci = find_seg(P.g_end, P.n_channels, e);
         const nlb_channel ch = P.chan[ci];
-        int64_t loc = e - ch.gb_off;
-        const int nhp = ch.nh1 * ch.nh2;
-        const int64_t n_gb = (int64_t)ch.np1 * ch.nh2 * nhp;
-        const T* Bc = B + ch.offset;
+        const int rowlen = ch.np2 * ch.nh1 * ch.nh2;
+        const int loc = (int)(e - ch.ga_off);
+        const int kq = loc / rowlen, rem = loc - kq * rowlen;
+        const int row = ch.hb1 + kq;
+        const T* Bc = B + ch.offset + rem;
         T acc = T(0);
-        if (loc < n_gb) {
-            const int hp = (int)(loc % nhp);
-            const int64_t r = loc / nhp;
-            const int kq = (int)(r % ch.nh2), ap = (int)(r / ch.nh2);
-            const int row = ch.hb2 + kq;
-            for (int q = P.fph_ptr[row]; q < P.fph_ptr[row + 1]; ++q)
-                acc += (T)P.fph_val[q] * Bc[((int64_t)ap * ch.np2 + P.fph_col[q]) * nhp + hp];
-        } else {
-            loc -= n_gb;
-            const int hp = (int)(loc % nhp);
-            const int64_t r = loc / nhp;
-            const int kq = (int)(r % ch.nh1), bp = (int)(r / ch.nh1);
-            const int row = ch.hb1 + kq;
-            for (int q = P.fph_ptr[row]; q < P.fph_ptr[row + 1]; ++q)
-                acc += (T)P.fph_val[q] * Bc[((int64_t)P.fph_col[q] * ch.np2 + bp) * nhp + hp];
-        }
+        for (int q = P.fph_ptr[row]; q < P.fph_ptr[row + 1]; ++q)
+            acc += (T)P.fph_val[q] * Bc[(int64_t)P.fph_col[q] * rowlen];
         G[e] = acc;
     }
 }
 
 // --------------------------------------------------------- T2 update ----
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_t2_update(nlb_struct_problem P, nlb_struct_state S) {
+// One block per row task (channel, a').  The row B[a'][:][:] is staged in
+// shared memory; everything along b, i and j reads it from there.  Only the
+// terms along a (f_pp neighbours of a' and the Ga rows) read other rows,
+// which sit in L2.  Per row the block also forms Gb[k'][i'j'] = sum_c f_ck
+// B[a'][c'][i'j'] (rank-h part of X_pp along b) and the T1 Fock term
+// F2[a'][i'] = sum_k' Gb[k'][i'k'].
+//
+// A thread owns work items (b', i') and walks j' (NH > 0: every label has NH
+// holes, the j' loop is unrolled and the per-item lists live in registers;
+// NH == 0: any hole counts).
+constexpr int kMaxNb = 8;   // stencil entries kept in registers (lattice: <= 7)
+
+template <typename T, int NH>
+__global__ void __launch_bounds__(kRowThreads, 2) k_t2_rows(nlb_struct_problem P, nlb_struct_state S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING || c->ccs) return;
     const int par = c->parity;
     const T* __restrict__ B = static_cast<const T*>(S.t2[par]);
     T* __restrict__ Bo = static_cast<T*>(S.t2[par ^ 1]);
-    const double* __restrict__ t1 = S.t1[par];
-    const int h = P.h;
-    const double* Xh2 = S.prep + (int64_t)h * h;
-    const double* dXp2 = S.prep + 3 * (int64_t)h * h;
-    const T* __restrict__ G = static_cast<const T*>(S.g);
+    const T* __restrict__ Ga = static_cast<const T*>(S.g);
+    T* __restrict__ F2 = static_cast<T*>(S.f2);
+    const PrepView V = prep_view(S.prep, P);
     T* E2 = (S.diis_t2 != nullptr && c->max_diis > 0 && c->diis_count < c->max_diis)
                 ? static_cast<T*>(S.diis_t2) + (int64_t)c->diis_count * P.n_t2 : nullptr;
     const T m = (T)c->mixing, om = (T)(1.0 - c->mixing);
+    const int mh = P.max_nh;
+    const bool diag_lad = NH > 0 && P.diag_ladders;
+    T* srow = reinterpret_cast<T*>(smem_raw);   // [max_row]  the row B[a']
+    T* sacc = srow + P.max_row;                 // [max_row]  terms along a
+    T* sgb = sacc + P.max_row;                  // [max_nh^3] Gb
+    T* sx1 = sgb + mh * mh * mh;                // [max_nh^2] X_hh of label g1
+    T* sx2 = sx1 + mh * mh;                     // [max_nh^2] X_hh of label g2
+    T* st1a = sx2 + mh * mh;                    // [max_nh]   t1[a, H_g1]
+    T* shh = st1a + mh;                         // [max_nh^2] diagonal hole-hole ladder
+    T* sdh2 = shh + mh * mh;                    // [max_nh]   diag X_hh of label g2
     double nrm = 0.0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < P.n_t2; e += stride) {
-        const int ci = find_seg(P.t2_end, P.n_channels, e);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int64_t task = blockIdx.x; task < P.n_rows; task += gridDim.x) {
+        const int ci = find_seg(P.row_end, P.n_channels, task);
         const nlb_channel ch = P.chan[ci];
-        const int64_t loc = e - ch.offset;
-        const int nh1 = ch.nh1, nh2 = ch.nh2, np2 = ch.np2;
+        const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
+        const int nh1 = NH ? NH : ch.nh1, nh2 = NH ? NH : ch.nh2, np2 = ch.np2;
         const int nhp = nh1 * nh2;
-        const int hp = (int)(loc % nhp);
-        const int64_t ab = loc / nhp;
-        const int bp = (int)(ab % np2), ap = (int)(ab / np2);
-        const int ip = hp / nh2, jp = hp % nh2;
-        const int a = P.p_ord[ch.pb1 + ap], b = P.p_ord[ch.pb2 + bp];
-        const int i = P.h_ord[ch.hb1 + ip], j = P.h_ord[ch.hb2 + jp];
-        const T* Bc = B + ch.offset;
-        const T* row = Bc + ab * nhp;
-        const T x = row[hp];
-        T R = T(0);
-        // f_pp along b and along a
-        const int rb = ch.pb2 + bp;
-        for (int q = P.fpp_ptr[rb]; q < P.fpp_ptr[rb + 1]; ++q)
-            R += (T)P.fpp_val[q] * Bc[((int64_t)ap * np2 + P.fpp_col[q]) * nhp + hp];
-        const int ra = ch.pb1 + ap;
-        for (int q = P.fpp_ptr[ra]; q < P.fpp_ptr[ra + 1]; ++q)
-            R += (T)P.fpp_val[q] * Bc[((int64_t)P.fpp_col[q] * np2 + bp) * nhp + hp];
-        // rank-h part of X_pp: -t1_bk Gb[a',k'] - t1_ak Ga[b',k']
-        const T* Gb = G + ch.gb_off + (int64_t)ap * nh2 * nhp + hp;
-        for (int kq = 0; kq < nh2; ++kq)
-            R -= (T)t1[(int64_t)b * h + P.h_ord[ch.hb2 + kq]] * Gb[(int64_t)kq * nhp];
-        const T* Ga = G + ch.ga_off + (int64_t)bp * nh1 * nhp + hp;
-        for (int kq = 0; kq < nh1; ++kq)
-            R -= (T)t1[(int64_t)a * h + P.h_ord[ch.hb1 + kq]] * Ga[(int64_t)kq * nhp];
-        // X_hh along i and along j
-        for (int kq = 0; kq < nh1; ++kq)
-            R += (T)Xh2[(int64_t)P.h_ord[ch.hb1 + kq] * h + i] * row[kq * nh2 + jp];
-        for (int kq = 0; kq < nh2; ++kq)
-            R += (T)Xh2[(int64_t)P.h_ord[ch.hb2 + kq] * h + j] * row[ip * nh2 + kq];
-        // hole-hole ladder on tau
+        const int rowlen = np2 * nhp;
+        const int64_t rbase = ch.offset + (int64_t)ap * rowlen;
+        const T* __restrict__ Brow = B + rbase;
+        const int32_t* hptr = P.hh_ptr + ch.hh_ptr_off;
+        const int32_t* hcol = P.hh_col + ch.hh_col_off;
+        const double* hval = P.hh_val + ch.hh_col_off;
+        const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off;
+        const int32_t* pcol = P.pp_col + ch.pp_col_off;
+        const double* pval = P.pp_val + ch.pp_col_off;
+        for (int e = tid; e < rowlen; e += nt) srow[e] = Brow[e];
+        const int x1b = P.xc_base[ch.g1], x2b = P.xc_base[ch.g2];
+        for (int e = tid; e < nh1 * nh1; e += nt) sx1[e] = (T)V.xc[x1b + e];
+        for (int e = tid; e < nh2 * nh2; e += nt) sx2[e] = (T)V.xc[x2b + e];
+        const int t1a_b = P.t1c_base[ch.g1] + ap * nh1;
+        for (int e = tid; e < nh1; e += nt) st1a[e] = (T)V.t1c[t1a_b + e];
+        for (int e = tid; e < nh2; e += nt) sdh2[e] = (T)V.dhc[ch.hb2 + e];
+        if (diag_lad)
+            for (int e = tid; e < nhp; e += nt) shh[e] = (hptr[e + 1] > hptr[e]) ? (T)hval[hptr[e]] : T(0);
+        __syncthreads();
+        // Gb[k'][hp] = sum_c f_ck B[a'][c'][hp] for the holes k of label g2
+        for (int e = tid; e < nh2 * nhp; e += nt) {
+            const int kq = e / nhp, hp = e - kq * nhp;
+            const int row = ch.hb2 + kq;
+            T acc = T(0);
+            for (int q = P.fph_ptr[row]; q < P.fph_ptr[row + 1]; ++q)
+                acc += (T)P.fph_val[q] * srow[P.fph_col[q] * nhp + hp];
+            sgb[e] = acc;
+        }
+        // Phase A (one thread per element, coalesced): the terms along a,
+        // f_pp neighbours of a' in other rows and -t1_ak Ga[k'].
+        const T* __restrict__ Gac = Ga + ch.ga_off;
+        const T* __restrict__ Bch = B + ch.offset;
         {
-            const int32_t* ptr = P.hh_ptr + ch.hh_ptr_off;
-            const int32_t* col = P.hh_col + ch.hh_col_off;
-            const double* val = P.hh_val + ch.hh_col_off;
-            for (int q = ptr[hp]; q < ptr[hp + 1]; ++q) {
-                const int in = col[q];
-                const int kq = in / nh2, lq = in % nh2;
-                const T tau = row[in] + (T)(t1[(int64_t)a * h + P.h_ord[ch.hb1 + kq]] *
-                                            t1[(int64_t)b * h + P.h_ord[ch.hb2 + lq]]);
-                R += (T)val[q] * tau;
+            const int ra0 = P.fpp_ptr[ch.pb1 + ap], ra1 = P.fpp_ptr[ch.pb1 + ap + 1];
+            const int na = min(ra1 - ra0, kMaxNb);
+            int acol[kMaxNb];
+            T aval[kMaxNb];
+#pragma unroll
+            for (int q = 0; q < kMaxNb; ++q) {
+                acol[q] = q < na ? P.fpp_col[ra0 + q] : ap;
+                aval[q] = q < na ? (T)P.fpp_val[ra0 + q] : T(0);
+            }
+            __syncthreads();  // st1a / srow visible
+            for (int e = tid; e < rowlen; e += nt) {
+                T acc = T(0);
+#pragma unroll
+                for (int q = 0; q < kMaxNb; ++q)
+                    acc += aval[q] * ((acol[q] == ap) ? srow[e] : Bch[(int64_t)acol[q] * rowlen + e]);
+                for (int q = ra0 + kMaxNb; q < ra1; ++q) {
+                    const int col = P.fpp_col[q];
+                    acc += (T)P.fpp_val[q] * ((col == ap) ? srow[e] : Bch[(int64_t)col * rowlen + e]);
+                }
+                if (NH) {
+#pragma unroll
+                    for (int k = 0; k < (NH ? NH : 1); ++k) acc -= st1a[k] * Gac[(int64_t)k * rowlen + e];
+                } else {
+                    for (int k = 0; k < nh1; ++k) acc -= st1a[k] * Gac[(int64_t)k * rowlen + e];
+                }
+                sacc[e] = acc;
             }
         }
-        // particle-particle ladder on tau
-        {
-            const int32_t* ptr = P.pp_ptr + ch.pp_ptr_off;
-            const int32_t* col = P.pp_col + ch.pp_col_off;
-            const double* val = P.pp_val + ch.pp_col_off;
-            for (int q = ptr[ab]; q < ptr[ab + 1]; ++q) {
-                const int in = col[q];
-                const int cq = in / np2, dq = in % np2;
-                const T tau = Bc[(int64_t)in * nhp + hp] +
-                              (T)(t1[(int64_t)P.p_ord[ch.pb1 + cq] * h + i] *
-                                  t1[(int64_t)P.p_ord[ch.pb2 + dq] * h + j]);
-                R += (T)val[q] * tau;
+        __syncthreads();
+        for (int iq = tid; iq < nh1; iq += nt) {
+            T acc = T(0);
+            for (int kq = 0; kq < nh2; ++kq) acc += sgb[kq * nhp + iq * nh2 + kq];
+            F2[ch.f2_off + (int64_t)ap * nh1 + iq] = acc;
+        }
+        const double da = V.dpc[ch.pb1 + ap];
+        const int t1b_b = P.t1c_base[ch.g2];
+        if (diag_lad) {
+            // Phase B, fixed hole count and diagonal ladders: a thread owns (b', i')
+            // and keeps the j' vector in registers.
+            constexpr int NHc = NH ? NH : 1;
+            constexpr int NHP = NHc * NHc;
+            for (int w = tid; w < np2 * NHc; w += nt) {
+                const int bp = w / NHc, ip = w - bp * NHc;
+                const int base = bp * NHP + ip * NHc;
+                T r[NHc], R[NHc], t1b[NHc];
+#pragma unroll
+                for (int j = 0; j < NHc; ++j) {
+                    r[j] = srow[base + j];
+                    R[j] = sacc[base + j];
+                    t1b[j] = (T)V.t1c[t1b_b + bp * NHc + j];
+                }
+                // f_pp along b
+                const int rbi = ch.pb2 + bp;
+                const int rb0 = P.fpp_ptr[rbi], rb1 = P.fpp_ptr[rbi + 1];
+                for (int q = rb0; q < rb1; ++q) {
+                    const T v = (T)P.fpp_val[q];
+                    const T* src = srow + P.fpp_col[q] * NHP + ip * NHc;
+#pragma unroll
+                    for (int j = 0; j < NHc; ++j) R[j] += v * src[j];
+                }
+                // rank-h part of X_pp along b
+#pragma unroll
+                for (int k = 0; k < NHc; ++k) {
+                    const T t = t1b[k];
+                    const T* g = sgb + k * NHP + ip * NHc;
+#pragma unroll
+                    for (int j = 0; j < NHc; ++j) R[j] -= t * g[j];
+                }
+                // X_hh along i (other i' of the same b') and along j (registers)
+#pragma unroll
+                for (int k = 0; k < NHc; ++k) {
+                    const T xk = sx1[k * NHc + ip];
+                    const T* src = srow + bp * NHP + k * NHc;
+#pragma unroll
+                    for (int j = 0; j < NHc; ++j) R[j] += xk * src[j];
+                }
+#pragma unroll
+                for (int j = 0; j < NHc; ++j) {
+                    T acc = T(0);
+#pragma unroll
+                    for (int k = 0; k < NHc; ++k) acc += sx2[k * NHc + j] * r[k];
+                    R[j] += acc;
+                }
+                // both ladders are diagonal and act on tau = t2 + t1 t1
+                const int ab = ap * np2 + bp;
+                const int q0 = pptr[ab];
+                const T cpp = (pptr[ab + 1] > q0) ? (T)pval[q0] : T(0);
+                const T ta = st1a[ip];
+                const double dpart = da + V.dpc[ch.pb2 + bp];
+                const double dhi = V.dhc[ch.hb1 + ip];
+#pragma unroll
+                for (int j = 0; j < NHc; ++j) {
+                    const T tau = r[j] + ta * t1b[j];
+                    R[j] += (shh[ip * NHc + j] + cpp) * tau;
+                    const double dd = -(dpart + (dhi + (double)sdh2[j]));
+                    const T tn = r[j] + R[j] / (T)dd;
+                    const T out = m * r[j] + om * tn;
+                    Bo[rbase + base + j] = out;
+                    const T d = out - r[j];
+                    if (E2) E2[rbase + base + j] = d;
+                    nrm += (double)d * (double)d;
+                }
+            }
+        } else {
+            // Phase B, general: any hole count, ladders from their CSR lists.
+            for (int w = tid; w < np2 * nh1; w += nt) {
+                const int bp = w / nh1, ip = w - bp * nh1;
+                const int base = bp * nhp + ip * nh2;
+                const int rbi = ch.pb2 + bp;
+                const int rb0 = P.fpp_ptr[rbi], rb1 = P.fpp_ptr[rbi + 1];
+                const double dab = da + V.dpc[ch.pb2 + bp];
+                const double dhi = V.dhc[ch.hb1 + ip];
+                const int ab = ap * np2 + bp;
+                const int p0 = pptr[ab], p1 = pptr[ab + 1];
+                for (int jp = 0; jp < nh2; ++jp) {
+                    const int hp = ip * nh2 + jp;
+                    const int e = base + jp;
+                    const T x = srow[e];
+                    T R = sacc[e];
+                    for (int q = rb0; q < rb1; ++q) R += (T)P.fpp_val[q] * srow[P.fpp_col[q] * nhp + hp];
+                    for (int k = 0; k < nh2; ++k) R -= (T)V.t1c[t1b_b + bp * nh2 + k] * sgb[k * nhp + hp];
+                    for (int k = 0; k < nh1; ++k) R += sx1[k * nh1 + ip] * srow[bp * nhp + k * nh2 + jp];
+                    for (int k = 0; k < nh2; ++k) R += sx2[k * nh2 + jp] * srow[base + k];
+                    for (int q = hptr[hp]; q < hptr[hp + 1]; ++q) {
+                        const int in = hcol[q];
+                        const int kq = in / nh2, lq = in - kq * nh2;
+                        const T tl = (T)V.t1c[t1b_b + bp * nh2 + lq];
+                        R += (T)hval[q] * (srow[bp * nhp + in] + st1a[kq] * tl);
+                    }
+                    for (int q = p0; q < p1; ++q) {
+                        const int in = pcol[q];
+                        const int cq = in / np2, dq = in - cq * np2;
+                        const T bin = (in == ab) ? x : Bch[(int64_t)in * nhp + hp];
+                        const double tt =
+                            V.t1c[P.t1c_base[ch.g1] + cq * nh1 + ip] * V.t1c[t1b_b + dq * nh2 + jp];
+                        R += (T)pval[q] * (bin + (T)tt);
+                    }
+                    const double dd = -(dab + (dhi + V.dhc[ch.hb2 + jp]));
+                    const T tn = x + R / (T)dd;
+                    const T out = m * x + om * tn;
+                    Bo[rbase + e] = out;
+                    const T d = out - x;
+                    if (E2) E2[rbase + e] = d;
+                    nrm += (double)d * (double)d;
+                }
             }
         }
-        const double dd = -((dXp2[a] + dXp2[b]) + (Xh2[(int64_t)i * h + i] + Xh2[(int64_t)j * h + j]));
-        const T tn = x + R / (T)dd;
-        const T out = m * x + om * tn;
-        Bo[e] = out;
-        const T d = out - x;
-        if (E2) E2[e] = d;
-        nrm += (double)d * (double)d;
+        __syncthreads();
     }
     const double s = block_sum(nrm);
     if (threadIdx.x == 0) atomicAdd(&S.ctrl->dt2_sq, 4.0 * s);
 }
 
 // --------------------------------------------------------- T1 update ----
+// R1 = f_ph + F2 + f_pp t1 - t1 Q/2 + t1 X_hh(T1 eq); Jacobi + mixing;
+// energy sum_ai f_ai t1'_ai (coupled_cluster.py:342-414, 265-286).
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nlb_struct_state S) {
     nlb_ctrl* c = S.ctrl;
@@ -253,10 +457,9 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
     const double* t1 = S.t1[par];
     double* t1o = S.t1[par ^ 1];
     const int h = P.h, p = P.p;
-    const double* Q = S.prep;
-    const double* Xh1 = S.prep + 2 * (int64_t)h * h;
-    const double* dXp1 = S.prep + 3 * (int64_t)h * h + p;
-    const T* G = static_cast<const T*>(S.g);
+    const PrepView V = prep_view(S.prep, P);
+    const T* Ga = static_cast<const T*>(S.g);
+    const T* F2 = static_cast<const T*>(S.f2);
     double* E1 = (S.diis_t1 != nullptr && c->max_diis > 0 && c->diis_count < c->max_diis)
                      ? S.diis_t1 + (int64_t)c->diis_count * p * h : nullptr;
     const double m = c->mixing;
@@ -276,13 +479,13 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
         if (!c->ccs) {
             for (int cc = 0; cc < P.n_channels; ++cc) {
                 const nlb_channel ch = P.chan[cc];
-                const int nhp = ch.nh1 * ch.nh2;
                 if (ch.g1 == g) {
-                    const T* Gb = G + ch.gb_off + (int64_t)ap * ch.nh2 * nhp + ip * ch.nh2;
-                    for (int kq = 0; kq < ch.nh2; ++kq) H1 += (double)Gb[(int64_t)kq * nhp + kq];
+                    H1 += (double)F2[ch.f2_off + (int64_t)ap * ch.nh1 + ip];
                 } else if (ch.g2 == g) {
-                    const T* Ga = G + ch.ga_off + (int64_t)ap * ch.nh1 * nhp + ip;
-                    for (int kq = 0; kq < ch.nh1; ++kq) H1 += (double)Ga[(int64_t)kq * nhp + kq * ch.nh2];
+                    const int nhp = ch.nh1 * ch.nh2;
+                    const int64_t rowlen = (int64_t)ch.np2 * nhp;
+                    const T* g0 = Ga + ch.ga_off + (int64_t)ap * nhp + ip;
+                    for (int kq = 0; kq < ch.nh1; ++kq) H1 += (double)g0[kq * rowlen + kq * ch.nh2];
                 }
             }
         }
@@ -292,9 +495,9 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
             H1 += P.fpp_val[q] * t1[(int64_t)P.p_ord[pb + P.fpp_col[q]] * h + i];
         for (int k = 0; k < h; ++k) {
             const double tk = t1[(int64_t)a * h + k];
-            if (tk != 0.0) H1 += tk * (Xh1[(int64_t)k * h + i] - 0.5 * Q[(int64_t)k * h + i]);
+            if (tk != 0.0) H1 += tk * (V.Xh1[(int64_t)k * h + i] - 0.5 * V.Q[(int64_t)k * h + i]);
         }
-        const double D1 = -(dXp1[a] + Xh1[(int64_t)i * h + i]);
+        const double D1 = -(V.dXp1[a] + V.Xh1[(int64_t)i * h + i]);
         const double x = t1[idx];
         const double tn = x + H1 / D1;
         const double out = m * x + (1.0 - m) * tn;
@@ -352,37 +555,52 @@ __global__ void k_finish(nlb_ctrl* c) {
 // the dense t2 (four images per stored amplitude).
 constexpr int kMaxDiis = 10;
 
-template <typename T>
+template <typename T, int M>
 __global__ void __launch_bounds__(kThreads) k_diis_gram(nlb_struct_problem P, nlb_struct_state S) {
     nlb_ctrl* c = S.ctrl;
     if (!c->diis_pulse) return;
-    const int m = c->max_diis;
-    double acc[kMaxDiis * (kMaxDiis + 1) / 2];
-    for (int k = 0; k < kMaxDiis * (kMaxDiis + 1) / 2; ++k) acc[k] = 0.0;
+    constexpr int NP = M * (M + 1) / 2;
+    double acc[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc[k] = 0.0;
     const int64_t n1 = (int64_t)P.p * P.h;
     const int64_t n2 = c->ccs ? 0 : P.n_t2;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const T* E2 = static_cast<const T*>(S.diis_t2);
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n1 + n2; e += stride) {
-        double v[kMaxDiis];
+        double v[M];
         double w;
         if (e < n1) {
-            for (int s = 0; s < m; ++s) v[s] = S.diis_t1[(int64_t)s * n1 + e];
+#pragma unroll
+            for (int s = 0; s < M; ++s) v[s] = S.diis_t1[(int64_t)s * n1 + e];
             w = 1.0;
         } else {
-            for (int s = 0; s < m; ++s) v[s] = (double)E2[(int64_t)s * P.n_t2 + (e - n1)];
+#pragma unroll
+            for (int s = 0; s < M; ++s) v[s] = (double)E2[(int64_t)s * P.n_t2 + (e - n1)];
             w = 4.0;
         }
         int k = 0;
-        for (int s = 0; s < m; ++s)
-            for (int t = s; t < m; ++t) acc[k++] += w * v[s] * v[t];
+#pragma unroll
+        for (int s = 0; s < M; ++s)
+#pragma unroll
+            for (int t = s; t < M; ++t) acc[k++] += w * v[s] * v[t];
     }
-    int k = 0;
-    for (int s = 0; s < m; ++s)
-        for (int t = s; t < m; ++t) {
-            const double tot = block_sum(acc[k++]);
-            if (threadIdx.x == 0) atomicAdd(&c->gram[s * kMaxDiis + t], tot);
-        }
+    // warp reductions, then one shared-memory pass per warp
+    __shared__ double red[kThreads / 32][NP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        const double v = warp_sum(acc[k]);
+        if (lane == 0) red[wid][k] = v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < NP; k += blockDim.x) {
+        double tot = 0.0;
+        for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) tot += red[w2][k];
+        int s = 0, rem = k;
+        while (rem >= M - s) { rem -= M - s; ++s; }
+        atomicAdd(&c->gram[s * kMaxDiis + s + rem], tot);
+    }
 }
 
 // Bordered DIIS system [B/max|B|, -1; -1, 0] c = [0, -1], solved by Gaussian
@@ -446,15 +664,15 @@ __global__ void k_diis_solve(nlb_ctrl* c) {
     }
 }
 
-template <typename T>
+template <typename T, int M>
 __global__ void __launch_bounds__(kThreads) k_diis_extrap(nlb_struct_problem P, nlb_struct_state S) {
     const nlb_ctrl* c = S.ctrl;
     if (!c->diis_pulse || !c->diis_applied) return;
-    const int m = c->max_diis;
     const int par = c->parity;
     const double w0 = c->gram[0];
-    double w[kMaxDiis];
-    for (int s = 0; s < m; ++s) w[s] = c->gram[1 + s];
+    double w[M];
+#pragma unroll
+    for (int s = 0; s < M; ++s) w[s] = c->gram[1 + s];
     const int64_t n1 = (int64_t)P.p * P.h;
     const int64_t n2 = c->ccs ? 0 : P.n_t2;
     double* t1 = S.t1[par];
@@ -464,12 +682,14 @@ __global__ void __launch_bounds__(kThreads) k_diis_extrap(nlb_struct_problem P, 
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n1 + n2; e += stride) {
         if (e < n1) {
             double v = w0 * t1[e];
-            for (int s = 0; s < m; ++s) v += w[s] * S.diis_t1[(int64_t)s * n1 + e];
+#pragma unroll
+            for (int s = 0; s < M; ++s) v += w[s] * S.diis_t1[(int64_t)s * n1 + e];
             t1[e] = v;
         } else {
             const int64_t q = e - n1;
             double v = w0 * (double)t2[q];
-            for (int s = 0; s < m; ++s) v += w[s] * (double)E2[(int64_t)s * P.n_t2 + q];
+#pragma unroll
+            for (int s = 0; s < M; ++s) v += w[s] * (double)E2[(int64_t)s * P.n_t2 + q];
             t2[q] = (T)v;
         }
     }
@@ -562,28 +782,48 @@ int num_sms() {
     return g_num_sms;
 }
 
-// Resident blocks per SM of each kernel, queried once.
-struct OccEntry { const void* fn; int bps; };
+// Resident blocks per SM of each kernel (for a given dynamic smem), queried once.
+struct OccEntry { const void* fn; int64_t smem; int bps; };
 OccEntry g_occ[64];
 int g_nocc = 0;
 
-int blocks_per_sm(const void* fn) {
+int blocks_per_sm(const void* fn, int64_t smem, int threads = kThreads) {
     for (int k = 0; k < g_nocc; ++k)
-        if (g_occ[k].fn == fn) return g_occ[k].bps;
+        if (g_occ[k].fn == fn && g_occ[k].smem == smem) return g_occ[k].bps;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int bps = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kThreads, 0) != cudaSuccess || bps <= 0) bps = 2;
-    if (g_nocc < 64) g_occ[g_nocc++] = OccEntry{fn, bps};
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, (size_t)smem) != cudaSuccess || bps <= 0)
+        bps = 1;
+    if (g_nocc < 64) g_occ[g_nocc++] = OccEntry{fn, smem, bps};
     return bps;
 }
 
 // Persistent-style grid: as many blocks as fit at once, never more than the work.
 template <typename K>
 int grid_for(K kernel, int64_t work) {
-    const int bps = blocks_per_sm(reinterpret_cast<const void*>(kernel));
+    const int bps = blocks_per_sm(reinterpret_cast<const void*>(kernel), 0);
     int64_t full = (int64_t)num_sms() * bps;
     int64_t need = (work + kThreads - 1) / kThreads;
     if (need < 1) need = 1;
     return (int)(need < full ? need : full);
+}
+
+int64_t smem_bytes(const nlb_struct_problem* P, int dtype) {
+    const int64_t el = dtype == NLB_F64 ? 8 : 4;
+    const int64_t mh = P->max_nh;
+    return el * (2 * (int64_t)P->max_row + mh * mh * mh + 3 * mh * mh + 2 * mh);
+}
+
+int64_t g_smem_limit = 0;
+
+int64_t smem_limit() {
+    if (g_smem_limit == 0) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        g_smem_limit = v > 0 ? v : 227 * 1024;
+    }
+    return g_smem_limit;
 }
 
 int valid(const nlb_struct_problem* P, const nlb_struct_state* S) {
@@ -591,30 +831,72 @@ int valid(const nlb_struct_problem* P, const nlb_struct_state* S) {
     if (P->p <= 0 || P->h <= 0 || P->n_channels < 0) return fail(NLB_ERR_SIZE, "bad p/h/channels");
     if (S->dtype != NLB_F64 && S->dtype != NLB_F32) return fail(NLB_ERR_ARG, "dtype must be NLB_F64 or NLB_F32");
     if (!S->t1[0] || !S->t1[1] || !S->prep) return fail(NLB_ERR_ARG, "null t1/prep buffer");
-    if (P->n_t2 > 0 && (!S->t2[0] || !S->t2[1] || !S->g)) return fail(NLB_ERR_ARG, "null t2/g buffer");
+    if (P->n_t2 > 0 && (!S->t2[0] || !S->t2[1] || !S->g || !S->f2)) return fail(NLB_ERR_ARG, "null t2/g/f2 buffer");
+    if (P->n_t2 > 0 && smem_bytes(P, S->dtype) > smem_limit())
+        return fail(NLB_ERR_SIZE, "a T2 row does not fit in shared memory");
     return NLB_OK;
 }
 
 template <typename T>
-int step_t(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t st) {
-    const int64_t nprep = (int64_t)P->h * P->h + P->p;
-    k_prep<<<(unsigned)((nprep + kThreads - 1) / kThreads), kThreads, 0, st>>>(*P, *S);
-    if (P->n_t2 > 0) {
-        k_gterms<T><<<grid_for(k_gterms<T>, P->n_g), kThreads, 0, st>>>(*P, *S);
-        k_t2_update<T><<<grid_for(k_t2_update<T>, P->n_t2), kThreads, 0, st>>>(*P, *S);
+void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, cudaStream_t st) {
+    switch (stage) {
+        case NLB_STAGE_PREP: {
+            const int64_t nprep = (int64_t)P->h * P->h + 2 * (int64_t)P->p + P->n_t1c + P->n_xc + P->h;
+            k_prep<<<(unsigned)((nprep + kThreads - 1) / kThreads), kThreads, 0, st>>>(*P, *S);
+            break;
+        }
+        case NLB_STAGE_GTERMS:
+            if (P->n_t2 > 0) k_ga<T><<<grid_for(k_ga<T>, P->n_g), kThreads, 0, st>>>(*P, *S);
+            break;
+        case NLB_STAGE_T2:
+            if (P->n_t2 > 0) {
+                const int64_t sm = smem_bytes(P, sizeof(T) == 8 ? NLB_F64 : NLB_F32);
+                auto kern = P->uniform_nh == 7 ? k_t2_rows<T, 7> : P->uniform_nh == 1 ? k_t2_rows<T, 1>
+                                                                                         : k_t2_rows<T, 0>;
+                const int bps = blocks_per_sm(reinterpret_cast<const void*>(kern), sm, kRowThreads);
+                int64_t grid = (int64_t)num_sms() * bps;
+                if (grid > P->n_rows) grid = P->n_rows;
+                kern<<<(unsigned)grid, kRowThreads, (size_t)sm, st>>>(*P, *S);
+            }
+            break;
+        case NLB_STAGE_T1:
+            k_t1_update<T><<<grid_for(k_t1_update<T>, (int64_t)P->p * P->h), kThreads, 0, st>>>(*P, *S);
+            break;
+        default:
+            k_finish<<<1, 32, 0, st>>>(S->ctrl);
     }
-    k_t1_update<T><<<grid_for(k_t1_update<T>, (int64_t)P->p * P->h), kThreads, 0, st>>>(*P, *S);
-    k_finish<<<1, 32, 0, st>>>(S->ctrl);
-    return check_launch("nlb_struct_step");
 }
 
 template <typename T>
-int diis_t(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t st) {
+int step_t(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t st) {
+    for (int k = NLB_STAGE_PREP; k <= NLB_STAGE_FINISH; ++k) stage_t<T>(P, S, k, st);
+    return check_launch("nlb_struct_step");
+}
+
+template <typename T, int M>
+void diis_m(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t st) {
     const int64_t n = (int64_t)P->p * P->h + P->n_t2;
-    k_diis_gram<T><<<grid_for(k_diis_gram<T>, n), kThreads, 0, st>>>(*P, *S);
+    k_diis_gram<T, M><<<grid_for(k_diis_gram<T, M>, n), kThreads, 0, st>>>(*P, *S);
     k_diis_solve<<<1, 32, 0, st>>>(S->ctrl);
-    k_diis_extrap<T><<<grid_for(k_diis_extrap<T>, n), kThreads, 0, st>>>(*P, *S);
+    k_diis_extrap<T, M><<<grid_for(k_diis_extrap<T, M>, n), kThreads, 0, st>>>(*P, *S);
     k_diis_done<<<1, 32, 0, st>>>(S->ctrl);
+}
+
+template <typename T>
+int diis_t(const nlb_struct_problem* P, const nlb_struct_state* S, int m, cudaStream_t st) {
+    switch (m) {
+        case 1: diis_m<T, 1>(P, S, st); break;
+        case 2: diis_m<T, 2>(P, S, st); break;
+        case 3: diis_m<T, 3>(P, S, st); break;
+        case 4: diis_m<T, 4>(P, S, st); break;
+        case 5: diis_m<T, 5>(P, S, st); break;
+        case 6: diis_m<T, 6>(P, S, st); break;
+        case 7: diis_m<T, 7>(P, S, st); break;
+        case 8: diis_m<T, 8>(P, S, st); break;
+        case 9: diis_m<T, 9>(P, S, st); break;
+        case 10: diis_m<T, 10>(P, S, st); break;
+        default: return fail(NLB_ERR_ARG, "max_diis must be in [1, 10]");
+    }
     return check_launch("nlb_struct_diis");
 }
 
@@ -626,7 +908,16 @@ int nlb_version(void) { return 1; }
 
 const char* nlb_last_error(void) { return g_err; }
 
-int64_t nlb_struct_prep_len(int32_t p, int32_t h) { return 3 * (int64_t)h * h + 2 * (int64_t)p; }
+int64_t nlb_struct_prep_len(const nlb_struct_problem* prob) {
+    if (!prob) return 0;
+    return 3 * (int64_t)prob->h * prob->h + 3 * (int64_t)prob->p + prob->n_t1c + prob->n_xc + prob->h;
+}
+
+int64_t nlb_struct_smem_bytes(const nlb_struct_problem* prob, int32_t dtype) {
+    if (!prob) return 0;
+    const int64_t b = smem_bytes(prob, dtype);
+    return b <= smem_limit() ? b : 0;
+}
 
 int nlb_struct_ctrl_init(nlb_ctrl* ctrl, double eps, double mixing, int32_t max_steps, int32_t criterion,
                          int32_t max_diis, int32_t ccs, double e0, nlb_stream_t stream) {
@@ -644,12 +935,24 @@ int nlb_struct_step(const nlb_struct_problem* prob, const nlb_struct_state* st, 
     return st->dtype == NLB_F64 ? step_t<double>(prob, st, s) : step_t<float>(prob, st, s);
 }
 
-int nlb_struct_diis(const nlb_struct_problem* prob, const nlb_struct_state* st, nlb_stream_t stream) {
+int nlb_struct_stage(const nlb_struct_problem* prob, const nlb_struct_state* st, int32_t stage,
+                     nlb_stream_t stream) {
+    int rc = valid(prob, st);
+    if (rc) return rc;
+    if (stage < NLB_STAGE_PREP || stage > NLB_STAGE_FINISH) return fail(NLB_ERR_ARG, "bad stage");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (st->dtype == NLB_F64) stage_t<double>(prob, st, stage, s); else stage_t<float>(prob, st, stage, s);
+    return check_launch("nlb_struct_stage");
+}
+
+int nlb_struct_diis(const nlb_struct_problem* prob, const nlb_struct_state* st, int32_t max_diis,
+                    nlb_stream_t stream) {
     int rc = valid(prob, st);
     if (rc) return rc;
     if (!st->diis_t1 || (prob->n_t2 > 0 && !st->diis_t2)) return fail(NLB_ERR_ARG, "null DIIS ring");
+    if (max_diis < 1 || max_diis > kMaxDiis) return fail(NLB_ERR_ARG, "max_diis must be in [1, 10]");
     cudaStream_t s = (cudaStream_t)stream;
-    return st->dtype == NLB_F64 ? diis_t<double>(prob, st, s) : diis_t<float>(prob, st, s);
+    return st->dtype == NLB_F64 ? diis_t<double>(prob, st, max_diis, s) : diis_t<float>(prob, st, max_diis, s);
 }
 
 int nlb_struct_energy(const nlb_struct_problem* prob, const nlb_struct_state* st, double* e_out,

@@ -171,7 +171,15 @@ def pppp_ladders(idx, val, t1, t2):
     return l1, l2
 
 
+# Skip diagrams whose operand block is identically zero (they add exact
+# zeros).  The CPU-baseline timing turns this off so that the port does the
+# same work as the reference, which evaluates every diagram.
+SKIP_ZERO_BLOCKS = True
+
+
 def _nz(x):
+    if not SKIP_ZERO_BLOCKS:
+        return x is not None
     return x is not None and np.any(x)
 
 

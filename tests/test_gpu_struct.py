@@ -92,9 +92,9 @@ def test_mixed_precision_energy(tag):
     ref = float(g["tight_e"])
     _, (e, _, _), info = _solve(tag, eps=1e-12, maxSteps=3000, max_diis=8, precision="mixed",
                                 mixed_eps=1e-7)
-    assert info["status"] == "converged"
-    assert abs(info["mixed_energy"] - ref) <= 1e-6 * abs(ref)
-    assert abs(e - ref) <= 1e-10 * abs(ref)
+    assert info["status"] == "converged", info
+    assert abs(info["mixed_energy"] - ref) <= 1e-6 * abs(ref), (info, ref)
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref, info)
 
 
 def test_compact_output_and_torch_inputs():
