@@ -148,6 +148,25 @@ int nlb_struct_step(const nlb_struct_problem *prob, const nlb_struct_state *st,
 int nlb_struct_stage(const nlb_struct_problem *prob, const nlb_struct_state *st, int32_t stage,
                      nlb_stream_t stream);
 
+/* No counterpart in the reference.  The same step as nlb_struct_step for
+ * callers that cannot allocate device memory -- for example an application
+ * whose memory manager has already reserved the whole of HBM, or a
+ * latency-critical loop where cudaMalloc/cudaFree would synchronise the
+ * device.  The caller passes t1, t2, ctrl (and the optional DIIS rings) as
+ * usual; st->g, st->f2 and st->prep are ignored.  The step's scratch comes
+ * from a fixed 8 MiB array in device memory that every GPU loading this
+ * library holds until exit; a problem that needs more (see
+ * nlb_struct_noalloc_scratch_bytes) is rejected with NLB_ERR_SIZE.  The first
+ * call on a device looks up the array's device address, so make it before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU (other streams, other threads) race and must not be issued.  Nothing is
+ * allocated or freed. */
+int nlb_struct_step_noalloc(const nlb_struct_problem *prob, const nlb_struct_state *st,
+                            nlb_stream_t stream);
+/* Bytes of the static scratch nlb_struct_step_noalloc needs for this problem
+ * and dtype (-1 on bad arguments). */
+int64_t nlb_struct_noalloc_scratch_bytes(const nlb_struct_problem *prob, int32_t dtype);
+
 /* Pulsed DIIS of the torch solver (CCM/soa/coupled_cluster.py:522-567): when
  * ctrl->diis_pulse is set, build the Gram matrix of the stored error vectors
  * (FP64), solve the bordered system in FP64 on the device and extrapolate the

@@ -91,6 +91,10 @@ def lib():
     L.nlb_convert.argtypes = [c_void_p, c_int32, c_void_p, c_int32, c_int64, c_void_p]
     L.nlb_struct_unpack_t2.argtypes = [ctypes.POINTER(StructProblem), c_void_p, c_int32, c_void_p, c_void_p]
     L.nlb_struct_pack_t2.argtypes = [ctypes.POINTER(StructProblem), c_void_p, c_void_p, c_int32, c_void_p]
+    L.nlb_struct_step_noalloc.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(StructState), c_void_p]
+    L.nlb_struct_step_noalloc.restype = c_int32
+    L.nlb_struct_noalloc_scratch_bytes.argtypes = [ctypes.POINTER(StructProblem), c_int32]
+    L.nlb_struct_noalloc_scratch_bytes.restype = c_int64
     for name in ("nlb_struct_ctrl_init", "nlb_struct_step", "nlb_struct_diis", "nlb_struct_energy",
                  "nlb_convert", "nlb_struct_unpack_t2", "nlb_struct_pack_t2"):
         getattr(L, name).restype = c_int32

@@ -902,7 +902,84 @@ int diis_t(const nlb_struct_problem* P, const nlb_struct_state* S, int m, cudaSt
 
 }  // namespace
 
+// ------------------------------------------------ no-allocation variant ----
+// Scratch for nlb_struct_step_noalloc: the dressed-Fock tables, the Ga
+// intermediates and the T1 Fock-term partial sums of one step, carved from a
+// fixed array in device memory instead of caller-allocated buffers.  Every
+// GPU that loads this library holds these 8 MiB until the process exits.
+#define NLB_NOALLOC_SCRATCH_BYTES (8u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NLB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_scratch(void** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        snprintf(g_err, sizeof(g_err), "nlb_struct_step_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+        return NLB_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kMaxDevices) return fail(NLB_ERR_ARG, "nlb_struct_step_noalloc: device index out of range");
+    if (g_noalloc_addr[dev] == nullptr) {
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || ptr == nullptr) {
+            snprintf(g_err, sizeof(g_err), "nlb_struct_step_noalloc: cudaGetSymbolAddress: %s",
+                     cudaGetErrorString(e));
+            return NLB_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = ptr;
+    }
+    *out = g_noalloc_addr[dev];
+    return NLB_OK;
+}
+
+int64_t align256(int64_t b) { return (b + 255) & ~int64_t(255); }
+}  // namespace
+
 extern "C" {
+
+int64_t nlb_struct_noalloc_scratch_bytes(const nlb_struct_problem* prob, int32_t dtype) {
+    if (!prob || (dtype != NLB_F64 && dtype != NLB_F32)) return -1;
+    const int64_t el = dtype == NLB_F64 ? 8 : 4;
+    return align256(nlb_struct_prep_len(prob) * 8) + align256(prob->n_g * el) + align256(prob->n_f2 * el);
+}
+
+int nlb_struct_step_noalloc(const nlb_struct_problem* prob, const nlb_struct_state* st, nlb_stream_t stream) {
+    if (!prob || !st || !st->ctrl) return fail(NLB_ERR_ARG, "nlb_struct_step_noalloc: null problem/state");
+    if (st->dtype != NLB_F64 && st->dtype != NLB_F32) return fail(NLB_ERR_ARG, "nlb_struct_step_noalloc: bad dtype");
+    const int64_t need = nlb_struct_noalloc_scratch_bytes(prob, st->dtype);
+    if (need < 0 || need > (int64_t)NLB_NOALLOC_SCRATCH_BYTES) {
+        snprintf(g_err, sizeof(g_err),
+                 "nlb_struct_step_noalloc: problem needs %lld bytes of scratch, more than the %u-byte static "
+                 "array; use nlb_struct_step with caller-allocated buffers",
+                 (long long)need, NLB_NOALLOC_SCRATCH_BYTES);
+        return NLB_ERR_SIZE;
+    }
+    void* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    const int64_t el = st->dtype == NLB_F64 ? 8 : 4;
+    unsigned char* p = static_cast<unsigned char*>(base);
+    nlb_struct_state local = *st;
+    local.prep = reinterpret_cast<double*>(p);
+    p += align256(nlb_struct_prep_len(prob) * 8);
+    local.g = p;
+    p += align256(prob->n_g * el);
+    local.f2 = p;
+    // Nothing in the scratch has to start at zero: every step writes the
+    // tables, Ga and F2 before reading them, and the CCS mode reads neither.
+    rc = valid(prob, &local);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    return local.dtype == NLB_F64 ? step_t<double>(prob, &local, s) : step_t<float>(prob, &local, s);
+}
+
 
 int nlb_version(void) { return 1; }
 
