@@ -192,6 +192,67 @@ int nlb_struct_unpack_t2(const nlb_struct_problem *prob, const void *t2c, int32_
 int nlb_struct_pack_t2(const nlb_struct_problem *prob, const double *t2_dense, void *t2c,
                        int32_t dtype, nlb_stream_t stream);
 
+/* ---------------------------------------------------------------------
+ * General (dense) engine: the full factorised equation set of
+ * CCM/coupled_cluster.py:342-545 on dense FP64 tensors in the reference's
+ * layouts, for inputs without the closed-site label structure.
+ * --------------------------------------------------------------------- */
+
+/* C[m,n] = alpha * sum_k A[m,k] B[k,n] + beta * C[m,n], where m, n, k and the
+ * batch index b are multi-indices of up to four dimensions each with their
+ * own strides in A, B and C (every pairwise einsum of ccDgrams.py). */
+typedef struct {
+    int32_t nm, nn, nk, nb;
+    int64_t M, N, K, B;                      /* products of the extents */
+    int64_t ext_m[4], ext_n[4], ext_k[4], ext_b[4];
+    int64_t sa_m[4], sc_m[4];                /* strides of the m dims in A and C */
+    int64_t sb_n[4], sc_n[4];                /* n dims in B and C */
+    int64_t sa_k[4], sb_k[4];                /* k dims in A and B */
+    int64_t sa_b[4], sb_b[4], sc_b[4];       /* batch dims in A, B and C */
+} nlb_contract_desc;
+
+int nlb_contract_f64(const nlb_contract_desc *d, const double *A, const double *B, double *C,
+                     double alpha, double beta, nlb_stream_t stream);
+
+/* H += alpha * P(Z) on (p,p,h,h) tensors, P = 1, pAB, pIJ or pIJ pAB
+ * (perm 0..3; ccDgrams.py:193-213). */
+int nlb_antisym_acc_f64(const double *Z, double *H, int64_t p, int64_t h, int32_t perm,
+                        double alpha, nlb_stream_t stream);
+
+/* In place: H_abij <- ((H_abij - H_baij) - (H_abji - H_baji)) / 4, exact
+ * antisymmetry in floating point; identity on exactly antisymmetric H. */
+int nlb_antisym_project_f64(double *H, int64_t p, int64_t h, nlb_stream_t stream);
+
+/* v_ppph_dgrams (ccDgrams.py:13-45): r[0..6] zero-filled by the caller, rows
+ * idx[q] = (c,d,a,k) with value val[q]; repeated keys add up. */
+int nlb_ppph_intermediates_f64(const int64_t *idx, const double *val, int64_t nnz, const double *t1,
+                               const double *t2, int64_t p, int64_t h, double *const *r,
+                               nlb_stream_t stream);
+
+/* v_pppp_dgrams (ccDgrams.py:215-237): l1 += v t2[c,d], l2 += v t1[c] t1[d]. */
+int nlb_pppp_ladders_f64(const int64_t *idx, const double *val, int64_t nnz, const double *t1,
+                         const double *t2, int64_t p, int64_t h, double *l1, double *l2,
+                         nlb_stream_t stream);
+
+/* Jacobi steps with mixing for T1 and T2 (coupled_cluster.py:410-414,
+ * 538-545, 614-620); e1/e2 (optional) receive new - old. */
+int nlb_jacobi_f64(const double *t1, const double *H1, const double *t2, const double *H2,
+                   const double *xpp1, const double *xhh1, const double *xpp2, const double *xhh2,
+                   int64_t p, int64_t h, double mixing, double *t1_out, double *t2_out, double *e1,
+                   double *e2, nlb_stream_t stream);
+
+/* ccsd_energy (coupled_cluster.py:265-286) into *out (device); v_pphh may be
+ * NULL when it is zero. */
+int nlb_dense_energy_f64(const double *f_ph, const double *t1, const double *v_pphh,
+                         const double *t2, int64_t p, int64_t h, double *out, nlb_stream_t stream);
+
+/* Pulsed DIIS on concatenated amplitude vectors (soa/coupled_cluster.py:
+ * 533-561): Gram of m error vectors err[m][n], FP64 bordered solve, and
+ * out = sum_s c_s hist[s] (out untouched when the solve fails).  work holds
+ * 512 doubles. */
+int nlb_vec_diis_f64(const double *err, const double *hist, int64_t n, int32_t m, double *work,
+                     double *out, nlb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,13 @@ class StructState(ctypes.Structure):
                 ("diis_t1", c_void_p), ("diis_t2", c_void_p), ("ctrl", c_void_p), ("dtype", c_int32)]
 
 
+class ContractDesc(ctypes.Structure):
+    _fields_ = [(n, c_int32) for n in ("nm", "nn", "nk", "nb")] + \
+               [(n, c_int64) for n in ("M", "N", "K", "B")] + \
+               [(n, c_int64 * 4) for n in ("ext_m", "ext_n", "ext_k", "ext_b", "sa_m", "sc_m", "sb_n", "sc_n",
+                                           "sa_k", "sb_k", "sa_b", "sb_b", "sc_b")]
+
+
 _lib = None
 _load_error = None
 
@@ -97,6 +104,21 @@ def lib():
     L.nlb_struct_noalloc_scratch_bytes.restype = c_int64
     for name in ("nlb_struct_ctrl_init", "nlb_struct_step", "nlb_struct_diis", "nlb_struct_energy",
                  "nlb_convert", "nlb_struct_unpack_t2", "nlb_struct_pack_t2"):
+        getattr(L, name).restype = c_int32
+    L.nlb_contract_f64.argtypes = [ctypes.POINTER(ContractDesc), c_void_p, c_void_p, c_void_p, c_double, c_double,
+                                   c_void_p]
+    L.nlb_antisym_acc_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int64, c_int32, c_double, c_void_p]
+    L.nlb_ppph_intermediates_f64.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_int64,
+                                             c_void_p, c_void_p]
+    L.nlb_pppp_ladders_f64.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_int64,
+                                       c_void_p, c_void_p, c_void_p]
+    L.nlb_jacobi_f64.argtypes = [c_void_p] * 8 + [c_int64, c_int64, c_double] + [c_void_p] * 5
+    L.nlb_dense_energy_f64.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]
+    L.nlb_antisym_project_f64.argtypes = [c_void_p, c_int64, c_int64, c_void_p]
+    L.nlb_antisym_project_f64.restype = c_int32
+    L.nlb_vec_diis_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]
+    for name in ("nlb_contract_f64", "nlb_antisym_acc_f64", "nlb_ppph_intermediates_f64", "nlb_pppp_ladders_f64",
+                 "nlb_jacobi_f64", "nlb_dense_energy_f64", "nlb_vec_diis_f64"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

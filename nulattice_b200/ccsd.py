@@ -27,6 +27,7 @@ Extra keyword-only arguments (not in the reference):
                DIIS, as the NumPy solver whose DIIS branch never fires).
 ``t2_format``  ``"dense"`` (default, reference layout) or ``"compact"``.
 ``info``       a dict to fill with status, iterations, engine and timings.
+``engine``     ``"auto"`` (default), ``"structured"`` or ``"general"``.
 """
 from __future__ import annotations
 
@@ -324,7 +325,7 @@ def _mp2_t1(f_pp, f_ph, f_hh, delta):
 def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10,
                 delta=0, mixing=0.5, verbose=False, sparse=True, ccs=False, device=None,
                 dtype=torch.float64, *, precision="fp64", criterion="soa", t2_format="dense",
-                mixed_eps=None, info=None):
+                mixed_eps=None, info=None, engine="auto"):
     """Solve the CCSD equations; returns ``(E_corr, t1, t2)``.
 
     Arguments as ``CCM/soa/coupled_cluster.py:440-454``: ``fock_mats`` =
@@ -352,7 +353,14 @@ def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000
         raise ValueError("mixing must be in [0, 1]")
     want_torch = isinstance(fock_mats[0], torch.Tensor)
     _lib.lib()  # fail loudly before any work when the library is missing
-    plan, why = _structure.detect(fock_mats, two_body_int, t1initial)
+    if engine not in ("auto", "structured", "general"):
+        raise ValueError("engine must be 'auto', 'structured' or 'general'")
+    if engine == "general":
+        plan, why = None, "general engine requested"
+    else:
+        plan, why = _structure.detect(fock_mats, two_body_int, t1initial)
+        if plan is None and engine == "structured":
+            raise ValueError(f"structured engine does not apply: {why}")
     if info is None:
         info = {}
     info["t_setup_start"] = t_start

@@ -31,6 +31,8 @@
 
 static thread_local char g_err[512] = "";
 
+void nlb_internal_set_error(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+
 static int fail(int code, const char* msg) {
     snprintf(g_err, sizeof(g_err), "%s", msg);
     return code;

@@ -1,0 +1,95 @@
+"""General (dense) CUDA engine vs the reference's golden vectors."""
+import numpy as np
+import pytest
+import torch
+
+import golden_io as G
+from nulattice_b200 import ccsd_solver
+from nulattice_b200 import dense as D
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda", 0)
+
+
+@pytest.fixture(scope="module")
+def rnd():
+    return G.load("dgrams_random")
+
+
+def _perm(x, perm):
+    if perm in (1, 3):
+        x = x - x.permute(1, 0, 2, 3)
+    if perm in (2, 3):
+        x = x - x.permute(0, 1, 3, 2)
+    return x
+
+
+@pytest.mark.parametrize("name", sorted(D.TERMS))
+def test_each_diagram(rnd, name):
+    coef, spec, names, perm = D.TERMS[name]
+    alias = {"r3": "x_pp", "r4": "x_pphh", "r5": "x_phhh", "r6": "x_phhh"}
+    ops = [torch.as_tensor(rnd[alias.get(n, n)], device=DEV) for n in names]
+    oz = spec.split("->")[1]
+    sizes = {}
+    for t, o in zip(spec.split("->")[0].split(","), ops):
+        for x, s in zip(t, o.shape):
+            sizes[x] = s
+    out = torch.empty([sizes[x] for x in oz], dtype=torch.float64, device=DEV)
+    E = D.GpuEinsum(torch.cuda.current_stream(DEV).cuda_stream)
+    E(spec, *ops, out=out, alpha=coef)
+    got = _perm(out, perm).cpu().numpy() if perm else out.cpu().numpy()
+    np.testing.assert_allclose(got, rnd["out_" + name], rtol=1e-10, atol=1e-10)
+
+
+def test_full_step_all_blocks(rnd):
+    fock = [rnd["f_pp"], rnd["f_ph"], rnd["f_hh"]]
+    two = [G.rows(rnd, "v_pppp"), G.rows(rnd, "v_ppph"), rnd["v_pphh"], rnd["v_phph"], rnd["v_phhh"], rnd["v_hhhh"]]
+    eng = D.DenseEngine(fock, two, DEV)
+    t1 = torch.as_tensor(rnd["t1"], device=DEV)
+    t2 = torch.as_tensor(rnd["t2"], device=DEV)
+    h1, xpp1, xhh1, h2, xpp2, xhh2 = eng.residuals(t1, t2)
+    n1 = t1 + h1 / -(torch.diagonal(xpp1)[:, None] + torch.diagonal(xhh1)[None, :])
+    dp, dh = torch.diagonal(xpp2), torch.diagonal(xhh2)
+    den = -(dp[:, None, None, None] + dp[None, :, None, None] + dh[None, None, :, None] + dh[None, None, None, :])
+    n2 = t2 + h2 / den
+    np.testing.assert_allclose(n1.cpu().numpy(), rnd["out_t1Iter"], rtol=1e-11, atol=1e-11)
+    np.testing.assert_allclose(n2.cpu().numpy(), rnd["out_t2Iter"], rtol=1e-11, atol=1e-10)
+    e = torch.zeros(1, dtype=torch.float64, device=DEV)
+    eng.energy(t1, t2, e)
+    assert float(e.item()) == pytest.approx(float(rnd["out_energy"]), rel=1e-12)
+
+
+@pytest.mark.parametrize("tag", ["he3_L3", "li6x_L3", "he4_L3_c1"])
+def test_trajectory_general_engine(tag):
+    g = G.load(tag)
+    fock, two = G.hamiltonian(g)
+    info = {}
+    e, t1, t2 = ccsd_solver(fock, two, eps=0.0, maxSteps=int(g["traj_steps"]), max_diis=0, device=DEV,
+                            criterion="numpy", engine="general", info=info)
+    assert info["engine"] == "general"
+    assert e == pytest.approx(float(g["traj_e"]), rel=1e-12)
+    np.testing.assert_allclose(t1, g["traj_t1"], atol=1e-13)
+    np.testing.assert_allclose(t2, G.dense(g, "traj_t2"), atol=1e-13)
+
+
+@pytest.mark.parametrize("tag", ["he3_L3", "li6x_L3"])
+def test_tight_energy_general_engine(tag):
+    g = G.load(tag)
+    fock, two = G.hamiltonian(g)
+    info = {}
+    e, t1, t2 = ccsd_solver(fock, two, eps=float(g["tight_eps"]), maxSteps=5000, max_diis=0, device=DEV,
+                            criterion="numpy", info=info)
+    assert info["engine"] == "general" and info["status"] == "converged"
+    ref = float(g["tight_e"])
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
+    np.testing.assert_allclose(t1, g["tight_t1"], atol=1e-10)
+
+
+def test_pulsed_diis_general_engine():
+    d = G.load("soa_diis_he4_L3")
+    g = G.load("he4_L3_t5")
+    fock, two = G.hamiltonian(g)
+    for steps in (4, 9, 13):
+        e, t1, t2 = ccsd_solver(fock, two, eps=0.0, maxSteps=steps, max_diis=4, device=DEV, engine="general")
+        assert e == pytest.approx(float(d[f"diis_e_{steps}"]), rel=1e-11)
+        np.testing.assert_allclose(t1, d[f"diis_t1_{steps}"], atol=1e-11)
