@@ -233,7 +233,7 @@ def _three_body_no2b(rows, is_hole, loc, p, h):
     return de, df_pp, df_hh, conv
 
 
-def normal_ordered_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, kinetic=True):
+def normal_ordered_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, kinetic=1.0):
     """``get_norm_ordered_ham`` for the lattice contact Hamiltonian
     (``CCM/coupled_cluster.py:752-832`` with ``sparse=True, NO2B=True``).
 
@@ -241,7 +241,10 @@ def normal_ordered_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, kinetic=T
     ``(E_ref, [f_pp, f_ph, f_hh], [v_pppp, v_ppph, v_pphh, v_phph, v_phhh, v_hhhh])``
     where ``v_pppp``/``v_ppph`` are ``(N,5)`` row arrays and the other four blocks
     are dense arrays (``dense=True``) or :class:`Block` objects.
-    ``kinetic=False`` drops the kinetic energy (used for coupling derivatives).
+    ``kinetic`` scales the kinetic energy; the Fock traces are still added
+    only where a kinetic entry exists, so ``kinetic=0`` gives the derivative
+    of every block with respect to the couplings (all blocks are linear in
+    vT1, vS1 and w3).
     """
     hole, part = ph_split(holes, L)
     h, p = len(hole), len(part)
@@ -256,11 +259,10 @@ def normal_ordered_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, kinetic=T
     # Fock matrices: kinetic entry plus the hole trace of the two-body blocks,
     # only where a kinetic entry exists (CCM/coupled_cluster.py:56-95)
     T = np.zeros((n, n)); has_t = np.zeros((n, n), bool)
-    if kinetic:
-        kr = kinetic_rows(L)
-        ti, tj = kr[:, 0].astype(np.int64), kr[:, 1].astype(np.int64)
-        np.add.at(T, (ti, tj), kr[:, 2])
-        has_t[ti, tj] = True
+    kr = kinetic_rows(L)
+    ti, tj = kr[:, 0].astype(np.int64), kr[:, 1].astype(np.int64)
+    np.add.at(T, (ti, tj), float(kinetic) * kr[:, 2])
+    has_t[ti, tj] = True
     f_pp = T[np.ix_(part, part)] + np.einsum("aibi->ab", dense2["phph"])
     f_ph = T[np.ix_(part, hole)] + np.einsum("aibi->ab", dense2["phhh"])
     f_hh = T[np.ix_(hole, hole)] + np.einsum("aibi->ab", dense2["hhhh"])
