@@ -193,6 +193,36 @@ int nlb_struct_pack_t2(const nlb_struct_problem *prob, const double *t2_dense, v
                        int32_t dtype, nlb_stream_t stream);
 
 /* ---------------------------------------------------------------------
+ * Adjoint of the structured engine (no counterpart in the reference, which
+ * has no gradients): CC Lambda equations at converged amplitudes, FP64.
+ * --------------------------------------------------------------------- */
+typedef struct {
+    double *lam1[2];    /* [p*h] multipliers of the T1 equation (double-buffered) */
+    double *lam2[2];    /* [n_t2] multipliers of the compact T2 equation */
+    const double *t1;   /* converged t1 [p*h] */
+    const double *t2;   /* converged compact t2 [n_t2], FP64 */
+    double *prep;       /* [nlb_struct_prep_len] tables at the converged t1 (filled by init) */
+    double *ga;         /* [n_g] Ga of the converged t2 (filled by init) */
+    double *ha;         /* [n_g] scratch */
+    double *acc;        /* [nlb_lambda_acc_len] scratch; after a step it holds Y1, U, T */
+    nlb_ctrl *ctrl;
+} nlb_lambda_state;
+
+int64_t nlb_lambda_acc_len(const nlb_struct_problem *prob);
+/* Zero the multipliers, build the tables at (t1, t2), reset ctrl; tol is the
+ * relative step size of the multipliers that ends the iteration. */
+int nlb_lambda_init(const nlb_struct_problem *prob, const nlb_lambda_state *st, double tol,
+                    double mixing, int32_t max_steps, nlb_stream_t stream);
+/* One Jacobi step of the Lambda equations; does nothing once ctrl->status is
+ * not NLB_RUNNING, so the accumulators keep U = t1^T lam1 and T of the last
+ * step that ran. */
+int nlb_lambda_step(const nlb_struct_problem *prob, const nlb_lambda_state *st, nlb_stream_t stream);
+/* *out = <lam2, (dW + dV) tau> for diagonal derivative ladders
+ * dw[hh_ptr_off + hp], dv[pp_ptr_off + ab] (tau = t2 + t1 t1). */
+int nlb_lambda_coupling(const nlb_struct_problem *prob, const nlb_lambda_state *st, const double *dw,
+                        const double *dv, double *out, nlb_stream_t stream);
+
+/* ---------------------------------------------------------------------
  * General (dense) engine: the full factorised equation set of
  * CCM/coupled_cluster.py:342-545 on dense FP64 tensors in the reference's
  * layouts, for inputs without the closed-site label structure.

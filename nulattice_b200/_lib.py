@@ -55,6 +55,11 @@ class StructState(ctypes.Structure):
                 ("diis_t1", c_void_p), ("diis_t2", c_void_p), ("ctrl", c_void_p), ("dtype", c_int32)]
 
 
+class LambdaState(ctypes.Structure):
+    _fields_ = [("lam1", c_void_p * 2), ("lam2", c_void_p * 2)] + [
+        (n, c_void_p) for n in ("t1", "t2", "prep", "ga", "ha", "acc", "ctrl")]
+
+
 class ContractDesc(ctypes.Structure):
     _fields_ = [(n, c_int32) for n in ("nm", "nn", "nk", "nb")] + \
                [(n, c_int64) for n in ("M", "N", "K", "B")] + \
@@ -114,6 +119,15 @@ def lib():
                                        c_void_p, c_void_p, c_void_p]
     L.nlb_jacobi_f64.argtypes = [c_void_p] * 8 + [c_int64, c_int64, c_double] + [c_void_p] * 5
     L.nlb_dense_energy_f64.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]
+    L.nlb_lambda_acc_len.argtypes = [ctypes.POINTER(StructProblem)]
+    L.nlb_lambda_acc_len.restype = c_int64
+    L.nlb_lambda_init.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_double, c_double,
+                                  c_int32, c_void_p]
+    L.nlb_lambda_step.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_void_p]
+    L.nlb_lambda_coupling.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_void_p,
+                                      c_void_p, c_void_p, c_void_p]
+    for name in ("nlb_lambda_init", "nlb_lambda_step", "nlb_lambda_coupling"):
+        getattr(L, name).restype = c_int32
     L.nlb_antisym_project_f64.argtypes = [c_void_p, c_int64, c_int64, c_void_p]
     L.nlb_antisym_project_f64.restype = c_int32
     L.nlb_vec_diis_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]

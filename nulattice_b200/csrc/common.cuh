@@ -1,0 +1,157 @@
+// Device helpers shared by the structured kernels (ccsd_struct.cu) and the
+// adjoint kernels (lambda.cu).  Included inside an anonymous namespace.
+#pragma once
+
+__device__ __forceinline__ int find_seg(const int64_t* end, int n, int64_t e) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (e < end[mid]) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum; every thread of the block must call it.
+__device__ double block_sum(double v) {
+    __shared__ double s[32];
+    v = warp_sum(v);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) s[w] = v;
+    __syncthreads();
+    int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? s[threadIdx.x] : 0.0;
+    if (w == 0) v = warp_sum(v);
+    return v;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------- prep ----
+// Layout of the prep scratch (doubles), see nlb_struct_prep_len:
+//   Q[h*h]   Q[k,j] = sum_c f_ck t1_cj
+//   Xh2[h*h] X_hh of the T2 equation, -f_hh - Q      (coupled_cluster.py:505-513)
+//   Xh1[h*h] X_hh of the T1 equation, -f_hh - Q/2    (coupled_cluster.py:388-393)
+//   dXp2[p], dXp1[p]  diagonals of X_pp: f_aa - S_a, f_aa - S_a/2, S_a = sum_k f_ak t1_ak
+//   t1c[n_t1c]  t1[P_g[a'], H_g[k']] per label (a' major)
+//   xc[n_xc]    Xh2[H_g[k'], H_g[i']] per label (k' major)
+//   dpc[p]      dXp2 in label order
+//   dhc[h]      diag Xh2 in label order
+struct PrepView {
+    double *Q, *Xh2, *Xh1, *dXp2, *dXp1, *t1c, *xc, *dpc, *dhc;
+};
+
+__host__ __device__ inline PrepView prep_view(double* base, const nlb_struct_problem& P) {
+    const int64_t hh = (int64_t)P.h * P.h;
+    PrepView v;
+    v.Q = base;
+    v.Xh2 = v.Q + hh;
+    v.Xh1 = v.Xh2 + hh;
+    v.dXp2 = v.Xh1 + hh;
+    v.dXp1 = v.dXp2 + P.p;
+    v.t1c = v.dXp1 + P.p;
+    v.xc = v.t1c + P.n_t1c;
+    v.dpc = v.xc + P.n_xc;
+    v.dhc = v.dpc + P.p;
+    return v;
+}
+
+__device__ __forceinline__ int find_label(const int32_t* base, int G, int64_t u) {
+    int lo = 0, hi = G - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (u >= base[mid]) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Q[k,i] = sum_c f_ck t1_ci using the f_ph column list of hole k.
+__device__ __forceinline__ double q_entry(const nlb_struct_problem& P, const double* t1, int k, int i) {
+    const int g = P.h_label[k];
+    const int row = P.h_base[g] + P.h_loc[k];
+    const int pb = P.p_base[g];
+    double q = 0.0;
+    for (int e = P.fph_ptr[row]; e < P.fph_ptr[row + 1]; ++e)
+        q += P.fph_val[e] * t1[(int64_t)P.p_ord[pb + P.fph_col[e]] * P.h + i];
+    return q;
+}
+
+__device__ __forceinline__ double s_entry(const nlb_struct_problem& P, const double* t1, int a) {
+    double s = 0.0;
+    for (int k = 0; k < P.h; ++k) s += P.f_ph[(int64_t)a * P.h + k] * t1[(int64_t)a * P.h + k];
+    return s;
+}
+
+// One thread of the prep tables (layout above) at amplitudes t1.
+__device__ void prep_body(const nlb_struct_problem& P, const double* t1, double* prep, int64_t u) {
+    const int h = P.h, p = P.p, G = P.n_labels;
+    const PrepView V = prep_view(prep, P);
+    const int64_t hh = (int64_t)h * h;
+    if (u < hh) {
+        const int k = (int)(u / h), j = (int)(u % h);
+        const double q = q_entry(P, t1, k, j);
+        V.Q[u] = q;
+        V.Xh2[u] = -P.f_hh[u] - q;
+        V.Xh1[u] = -P.f_hh[u] - 0.5 * q;
+        return;
+    }
+    u -= hh;
+    if (u < p) {
+        const double s = s_entry(P, t1, (int)u);
+        V.dXp2[u] = P.fpp_diag[u] - s;
+        V.dXp1[u] = P.fpp_diag[u] - 0.5 * s;
+        return;
+    }
+    u -= p;
+    if (u < P.n_t1c) {
+        const int g = find_label(P.t1c_base, G, u);
+        const int nh = P.h_base[g + 1] - P.h_base[g];
+        const int loc = (int)(u - P.t1c_base[g]);
+        const int ap = loc / nh, kq = loc - ap * nh;
+        V.t1c[u] = t1[(int64_t)P.p_ord[P.p_base[g] + ap] * h + P.h_ord[P.h_base[g] + kq]];
+        return;
+    }
+    u -= P.n_t1c;
+    if (u < P.n_xc) {
+        const int g = find_label(P.xc_base, G, u);
+        const int nh = P.h_base[g + 1] - P.h_base[g];
+        const int loc = (int)(u - P.xc_base[g]);
+        const int kq = loc / nh, iq = loc - kq * nh;
+        const int k = P.h_ord[P.h_base[g] + kq], i = P.h_ord[P.h_base[g] + iq];
+        V.xc[u] = -P.f_hh[(int64_t)k * h + i] - q_entry(P, t1, k, i);
+        return;
+    }
+    u -= P.n_xc;
+    if (u < p) {
+        const int a = P.p_ord[u];
+        V.dpc[u] = P.fpp_diag[a] - s_entry(P, t1, a);
+        return;
+    }
+    u -= p;
+    if (u < h) {
+        const int i = P.h_ord[u];
+        V.dhc[u] = -P.f_hh[(int64_t)i * h + i] - q_entry(P, t1, i, i);
+    }
+}
+
+
+// Ga[k'][b'][i'j'] = sum_c f_ck B[c'][b'][i'j'] (k = hole k' of label g1) at
+// flat index e of the Ga array: the f_ph^T t2 half-contraction along the
+// first particle index.  With t1 it gives the rank-h part of X_pp t2 along a,
+// and it holds the T1 Fock term f_ck t2_acik for particles of label g2.
+template <typename T>
+__device__ __forceinline__ T ga_element(const nlb_struct_problem& P, const T* B, int64_t e) {
+    const int ci = find_seg(P.g_end, P.n_channels, e);
+    const nlb_channel ch = P.chan[ci];
+    const int rowlen = ch.np2 * ch.nh1 * ch.nh2;
+    const int loc = (int)(e - ch.ga_off);
+    const int kq = loc / rowlen, rem = loc - kq * rowlen;
+    const int row = ch.hb1 + kq;
+    const T* Bc = B + ch.offset + rem;
+    T acc = T(0);
+    for (int q = P.fph_ptr[row]; q < P.fph_ptr[row + 1]; ++q) acc += (T)P.fph_val[q] * Bc[(int64_t)P.fph_col[q] * rowlen];
+    return acc;
+}
