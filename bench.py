@@ -288,7 +288,7 @@ def main():
     tfile = os.path.join(ROOT, "profiles", "t2_update_traffic.json")
     if os.path.exists(tfile):
         traffic = json.load(open(tfile)).get("bytes_per_launch")
-    roofline = {"kernel": "k_t2_rows<float, 7>", "bound": "hbm", "achieved": achieved, "peak": peak,
+    roofline = {"kernel": "k_t2_lat<float, 7, 256, 2>", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_us": k_ms * 1e3, "launches": len(m_k)}
 

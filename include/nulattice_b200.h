@@ -60,6 +60,8 @@ typedef struct {
     int32_t max_nh;               /* max holes in one label */
     int32_t uniform_nh;           /* every channel has nh1 == nh2 == this (0: not uniform) */
     int32_t diag_ladders;         /* 1: both ladders only couple a pair to itself */
+    int32_t max_fpp_offdiag;      /* most off-diagonal entries in one f_pp row */
+    int32_t reserved;             /* 0 */
     const nlb_channel *chan;      /* [n_channels] */
     const int64_t *t2_end;        /* [n_channels] cumulative end of each block */
     const int64_t *g_end;         /* [n_channels] cumulative end of Ga blocks */

@@ -160,6 +160,12 @@ class StructuredEngine:
                 if np.any(cnt > 1) or np.any(col != rows_):
                     diag = False
         prob.diag_ladders = int(diag)
+        # off-diagonal f_pp entries per row (rows label-ordered, columns label-local)
+        fp = np.asarray(pl.fpp_ptr)
+        row_loc = np.concatenate([np.arange(len(x)) for x in pl.p_of]) if G else np.zeros(0, np.int64)
+        row_id = np.repeat(np.arange(len(fp) - 1), np.diff(fp))
+        offd = np.asarray(pl.fpp_col) != row_loc[row_id]
+        prob.max_fpp_offdiag = int(np.bincount(row_id[offd], minlength=1).max()) if offd.any() else 0
         for k, v in T.items():
             setattr(prob, k, v.data_ptr())
         self.prob = prob

@@ -307,6 +307,334 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_t2_rows(nlb_struct_problem P
     if (threadIdx.x == 0) atomicAdd(&S.ctrl->dt2_sq, 4.0 * s);
 }
 
+// ------------------------------------------------ T2 update, lattice path ----
+// Closed-site lattice inputs: every label has NH holes and both ladders only
+// couple a pair to itself.  Same residual as k_t2_rows, organised so that one
+// pass over the row does everything, coalesced over the row:
+//
+// * the block is NB = NT / NH^2 groups of NH^2 threads; a thread keeps one
+//   hole pair (i', j') for the whole row and its group walks b' = q, q + NB,
+//   ..., so the X_hh columns of i' and j', the hole-hole ladder entry and the
+//   hole part of the denominator are registers;
+// * rows arrive in shared memory by cp.async (16-byte copies for the aligned
+//   middle, element copies for the ragged ends), double-buffered: the next
+//   row is in flight while the block works on the current one;
+// * per-b' data sits next to the row in 32-byte records read with vector
+//   loads: t1[b', H_g2] and the particle-particle ladder entry of (a', b'),
+//   the f_pp row of b' as pre-scaled offsets and values;
+// * the terms along a (f_pp neighbours of a' and the Ga rows) are read from
+//   L2 with one coalesced load per term, issued one b' step ahead; the
+//   neighbour rows of consecutive a' overlap because each block takes a
+//   contiguous range of rows.
+//
+// Launched only when every f_pp row has at most kLatNa off-diagonal entries
+// (max_fpp_offdiag), so the f_pp row of b' with its diagonal fits the
+// kLatNb - 1 used slots of its record.
+constexpr int kLatNb = 8;    // record slots per b' (at most 7 used)
+constexpr int kLatNa = 6;    // off-diagonal f_pp entries of a' kept in registers
+
+struct LatSmem {
+    int64_t row0, row1, gb, rec, dp, off, val, total;
+};
+
+__host__ __device__ inline int64_t lat_round16(int64_t b) { return (b + 15) & ~int64_t(15); }
+
+// Shared-memory layout of k_t2_lat for element size el and NH holes per label.
+__host__ __device__ inline LatSmem lat_smem(int64_t max_row, int nh, int64_t el) {
+    const int64_t np2 = max_row / (nh * nh);
+    const int64_t rowb = lat_round16(el * (max_row + 16 / el + 4));
+    LatSmem s;
+    s.row0 = 0;
+    s.row1 = rowb;
+    s.gb = 2 * rowb;
+    s.rec = s.gb + lat_round16(el * nh * nh * nh);
+    s.dp = s.rec + lat_round16(el * np2 * kLatNb);
+    s.off = s.dp + lat_round16(el * np2);
+    s.val = s.off + lat_round16(4 * np2 * kLatNb);
+    s.total = s.val + lat_round16(el * np2 * kLatNb);
+    return s;
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_el(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Eight consecutive shared-memory values (16-byte aligned) with vector loads.
+__device__ __forceinline__ void lds8(const float* p, float (&v)[8]) {
+    const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void lds8(const double* p, double (&v)[8]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double2 a = reinterpret_cast<const double2*>(p)[k];
+        v[2 * k] = a.x; v[2 * k + 1] = a.y;
+    }
+}
+__device__ __forceinline__ void lds8(const int32_t* p, int (&v)[8]) {
+    const int4 a = reinterpret_cast<const int4*>(p)[0], b = reinterpret_cast<const int4*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+
+// Jacobi quotient R / D.  FP32 amplitudes: the approximate reciprocal (the
+// denominators only set the step length, the fixed point R = 0 does not
+// depend on them); FP64: IEEE division.
+__device__ __forceinline__ float lat_div(float r, float d) { return __fdividef(r, d); }
+__device__ __forceinline__ double lat_div(double r, double d) { return r / d; }
+
+// Queue the asynchronous copy of the row starting at `src` (rowlen elements)
+// into the buffer `dst`; returns the element shift that makes the 16-byte
+// copies aligned on both sides.
+template <typename T, int NT>
+__device__ __forceinline__ int lat_issue_row(T* dst, const T* src, int rowlen) {
+    constexpr int VEC = 16 / (int)sizeof(T);
+    const int mis = (int)((reinterpret_cast<uintptr_t>(src) / sizeof(T)) & (VEC - 1));
+    T* d = dst + mis;
+    const int head = min((VEC - mis) & (VEC - 1), rowlen);
+    const int nvec = (rowlen - head) / VEC;
+    const int tail0 = head + nvec * VEC;
+    for (int e = threadIdx.x; e < head; e += NT) cp_async_el<sizeof(T)>(d + e, src + e);
+    for (int v = threadIdx.x; v < nvec; v += NT) cp_async16(d + head + v * VEC, src + head + v * VEC);
+    for (int e = tail0 + threadIdx.x; e < rowlen; e += NT) cp_async_el<sizeof(T)>(d + e, src + e);
+    cp_async_commit();
+    return mis;
+}
+
+template <typename T, int NH, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_struct_state S) {
+    constexpr int NHP = NH * NH;
+    constexpr int NB = NT / NHP;
+    static_assert(NB >= 1 && NH <= 7, "block must hold one hole-pair group; a record holds 7 holes");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const nlb_ctrl* c = S.ctrl;
+    if (c->status != NLB_RUNNING || c->ccs) return;
+    const int par = c->parity;
+    const T* __restrict__ B = static_cast<const T*>(S.t2[par]);
+    T* __restrict__ Bo = static_cast<T*>(S.t2[par ^ 1]);
+    const T* __restrict__ Ga = static_cast<const T*>(S.g);
+    T* __restrict__ F2 = static_cast<T*>(S.f2);
+    const PrepView V = prep_view(S.prep, P);
+    T* E2 = (S.diis_t2 != nullptr && c->max_diis > 0 && c->diis_count < c->max_diis)
+                ? static_cast<T*>(S.diis_t2) + (int64_t)c->diis_count * P.n_t2 : nullptr;
+    const T m = (T)c->mixing, om = (T)(1.0 - c->mixing);
+    const LatSmem L = lat_smem(P.max_row, NH, sizeof(T));
+    T* sgb = reinterpret_cast<T*>(smem_raw + L.gb);        // Gb[k'][i'j'] of this row
+    T* srec = reinterpret_cast<T*>(smem_raw + L.rec);      // [b'][8]: t1[b', k'] (k' < NH), pp ladder at 7
+    T* sdp = reinterpret_cast<T*>(smem_raw + L.dp);        // [b']: particle part of the denominator
+    int32_t* soff = reinterpret_cast<int32_t*>(smem_raw + L.off);   // [b'][8] f_pp columns * NH^2
+    T* sval = reinterpret_cast<T*>(smem_raw + L.val);      // [b'][8] f_pp values (0 = padding)
+
+    const int tid = threadIdx.x;
+    const bool active = tid < NB * NHP;
+    const int grp = tid / NHP, hp = tid - grp * NHP;
+    const int ip = hp / NH, jp = hp - ip * NH;
+    double nrm = 0.0;
+    int cur_ci = -1;
+    T x1[NH], x2[NH], hh = T(0), dh = T(0);
+
+    const int64_t t0 = (int64_t)blockIdx.x * P.n_rows / gridDim.x;
+    const int64_t t1e = (int64_t)(blockIdx.x + 1) * P.n_rows / gridDim.x;
+    int ci = t0 < t1e ? find_seg(P.row_end, P.n_channels, t0) : 0;
+    int mis = 0;
+    if (t0 < t1e) {
+        const nlb_channel c0 = P.chan[ci];
+        const int ap0 = (int)(t0 - (ci ? P.row_end[ci - 1] : 0));
+        const int rl = c0.np2 * NHP;
+        mis = lat_issue_row<T, NT>(reinterpret_cast<T*>(smem_raw + L.row0), B + c0.offset + (int64_t)ap0 * rl, rl);
+    }
+    for (int64_t task = t0; task < t1e; ++task) {
+        const int buf = (int)((task - t0) & 1);
+        const nlb_channel ch = P.chan[ci];
+        const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
+        const int np2 = ch.np2;
+        const int rowlen = np2 * NHP;
+        const int64_t rbase = ch.offset + (int64_t)ap * rowlen;
+        // (shared addresses computed from smem_raw directly, never through a
+        // pointer array, so that every access stays a shared-memory access)
+        const T* srow = reinterpret_cast<const T*>(smem_raw + (buf ? L.row1 : L.row0)) + mis;
+
+        // per-channel tables (the block's rows are contiguous: usually unchanged)
+        if (ci != cur_ci) {
+            cur_ci = ci;
+            const int x1b = P.xc_base[ch.g1], x2b = P.xc_base[ch.g2];
+#pragma unroll
+            for (int k = 0; k < NH; ++k) {
+                x1[k] = (T)V.xc[x1b + k * NH + ip];
+                x2[k] = (T)V.xc[x2b + k * NH + jp];
+            }
+            const int32_t* hptr = P.hh_ptr + ch.hh_ptr_off;
+            hh = (hptr[hp + 1] > hptr[hp]) ? (T)P.hh_val[ch.hh_col_off + hptr[hp]] : T(0);
+            dh = (T)(V.dhc[ch.hb1 + ip] + V.dhc[ch.hb2 + jp]);
+            const int t1b_b = P.t1c_base[ch.g2];
+            for (int w = tid; w < np2 * kLatNb; w += NT) {
+                const int bp = w / kLatNb, k = w - bp * kLatNb;
+                if (k < NH) srec[w] = (T)V.t1c[t1b_b + bp * NH + k];
+                const int r0 = P.fpp_ptr[ch.pb2 + bp], r1 = P.fpp_ptr[ch.pb2 + bp + 1];
+                soff[w] = ((k < r1 - r0) ? P.fpp_col[r0 + k] : bp) * NHP;
+                sval[w] = (k < r1 - r0) ? (T)P.fpp_val[r0 + k] : T(0);
+            }
+        }
+        // per-row: a' stencil (off-diagonal part in registers; unused slots
+        // point at the row itself with weight 0), t1[a', H_g1], the pp ladder
+        // entries and particle denominators of the pairs (a', b')
+        const int ra0 = P.fpp_ptr[ch.pb1 + ap], ra1 = P.fpp_ptr[ch.pb1 + ap + 1];
+        T adiag = T(0);
+        int aoff[kLatNa];
+        T aval[kLatNa];
+        {
+            int q = ra0;
+#pragma unroll
+            for (int s = 0; s < kLatNa; ++s) {
+                aoff[s] = ap * rowlen;
+                aval[s] = T(0);
+                for (; q < ra1; ++q) {
+                    const int col = P.fpp_col[q];
+                    if (col == ap) { adiag += (T)P.fpp_val[q]; continue; }
+                    aoff[s] = col * rowlen;
+                    aval[s] = (T)P.fpp_val[q];
+                    ++q;
+                    break;
+                }
+            }
+            for (; q < ra1; ++q)
+                if (P.fpp_col[q] == ap) adiag += (T)P.fpp_val[q];
+        }
+        T t1a[NH];
+        const int t1a_b = P.t1c_base[ch.g1] + ap * NH;
+#pragma unroll
+        for (int k = 0; k < NH; ++k) t1a[k] = (T)V.t1c[t1a_b + k];
+        const T t1ai = (T)V.t1c[t1a_b + ip];
+        const double da = V.dpc[ch.pb1 + ap];
+        const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off;
+        const double* pval = P.pp_val + ch.pp_col_off;
+        for (int bp = tid; bp < np2; bp += NT) {
+            const int ab = ap * np2 + bp;
+            srec[bp * kLatNb + 7] = (pptr[ab + 1] > pptr[ab]) ? (T)pval[pptr[ab]] : T(0);
+            sdp[bp] = (T)(da + V.dpc[ch.pb2 + bp]);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        // next row in flight while this one is worked on (its buffer was last
+        // read by the row before, which ended with a barrier)
+        int next_ci = ci, next_mis = 0;
+        if (task + 1 < t1e) {
+            if (task + 1 >= P.row_end[ci]) ++next_ci;
+            const nlb_channel cn = P.chan[next_ci];
+            const int apn = (int)(task + 1 - (next_ci ? P.row_end[next_ci - 1] : 0));
+            const int rl = cn.np2 * NHP;
+            next_mis = lat_issue_row<T, NT>(reinterpret_cast<T*>(smem_raw + (buf ? L.row0 : L.row1)),
+                                            B + cn.offset + (int64_t)apn * rl, rl);
+        }
+        // Gb[k'][hp] = sum_c f_ck B[a'][c'][hp] (holes k of label g2), then F2
+        for (int e = tid; e < NH * NHP; e += NT) {
+            const int kq = e / NHP, h2 = e - kq * NHP;
+            const int row = ch.hb2 + kq;
+            T acc = T(0);
+            for (int q = P.fph_ptr[row]; q < P.fph_ptr[row + 1]; ++q)
+                acc += (T)P.fph_val[q] * srow[P.fph_col[q] * NHP + h2];
+            sgb[e] = acc;
+        }
+        __syncthreads();
+        if (tid < NH) {
+            T acc = T(0);
+#pragma unroll
+            for (int kq = 0; kq < NH; ++kq) acc += sgb[kq * NHP + tid * NH + kq];
+            F2[ch.f2_off + (int64_t)ap * NH + tid] = acc;
+        }
+        if (active && grp < np2) {
+            const T* __restrict__ gB = B + ch.offset + hp;
+            const T* __restrict__ gG = Ga + ch.ga_off + hp;
+            T* __restrict__ Bout = Bo + rbase + hp;
+            T* __restrict__ Eout = E2 ? E2 + rbase + hp : nullptr;
+            const T* s_hp = srow + hp;
+            const T* s_col = srow + jp;          // B[b'][k'][j'] at eb + k' NH
+            const T* s_row = srow + ip * NH;     // B[b'][i'][k'] at eb + k'
+            const T* g_hp = sgb + hp;
+            T nrm_row = T(0);
+            // one element (b', i', j') given its terms along a
+            auto element = [&](int bp, int eb, const T (&nb)[kLatNa], const T (&gv)[NH]) {
+                const T x = s_hp[eb];
+                T rec[8], sv[8];
+                int so[8];
+                lds8(srec + bp * kLatNb, rec);
+                lds8(soff + bp * kLatNb, so);
+                lds8(sval + bp * kLatNb, sv);
+                // f_pp along b
+                T accb = T(0);
+#pragma unroll
+                for (int q = 0; q < kLatNb - 1; ++q) accb += sv[q] * s_hp[so[q]];
+                // rank-h part along b: -t1_bk Gb[k]
+                T accg = T(0);
+#pragma unroll
+                for (int k = 0; k < NH; ++k) accg += rec[k] * g_hp[k * NHP];
+                // X_hh along i and along j
+                T accx = T(0), accy = T(0);
+#pragma unroll
+                for (int k = 0; k < NH; ++k) {
+                    accx += x1[k] * s_col[eb + k * NH];
+                    accy += x2[k] * s_row[eb + k];
+                }
+                // along a: f_pp neighbours and the rank-h part -t1_ak Ga[k]
+                T acca = adiag * x, accG = T(0);
+#pragma unroll
+                for (int q = 0; q < kLatNa; ++q) acca += aval[q] * nb[q];
+#pragma unroll
+                for (int k = 0; k < NH; ++k) accG += t1a[k] * gv[k];
+                // both ladders act on tau = t2 + t1 t1
+                const T t1bj = srec[bp * kLatNb + jp];
+                const T lad = (hh + rec[7]) * (x + t1ai * t1bj);
+                const T acc = ((acca - accG) + (accb - accg)) + ((accx + accy) + lad);
+                const T dd = -(sdp[bp] + dh);
+                const T tn = x + lat_div(acc, dd);
+                const T out = m * x + om * tn;
+                __stcg(Bout + eb, out);
+                const T d = out - x;
+                if (Eout) __stcg(Eout + eb, d);
+                nrm_row += d * d;
+            };
+            // the L2 loads of one b' step go out a step ahead of its math
+            T rnb[kLatNa], rgv[NH];
+            {
+                const int eb = grp * NHP;
+#pragma unroll
+                for (int q = 0; q < kLatNa; ++q) rnb[q] = __ldg(gB + aoff[q] + eb);
+#pragma unroll
+                for (int k = 0; k < NH; ++k) rgv[k] = __ldg(gG + k * rowlen + eb);
+            }
+            for (int bp = grp; bp < np2; bp += NB) {
+                const int eb = bp * NHP;
+                T nb[kLatNa], gv[NH];
+#pragma unroll
+                for (int q = 0; q < kLatNa; ++q) nb[q] = rnb[q];
+#pragma unroll
+                for (int k = 0; k < NH; ++k) gv[k] = rgv[k];
+                const int ebn = (bp + NB < np2) ? eb + NB * NHP : eb;
+#pragma unroll
+                for (int q = 0; q < kLatNa; ++q) rnb[q] = __ldg(gB + aoff[q] + ebn);
+#pragma unroll
+                for (int k = 0; k < NH; ++k) rgv[k] = __ldg(gG + k * rowlen + ebn);
+                element(bp, eb, nb, gv);
+            }
+            nrm += (double)nrm_row;
+        }
+        __syncthreads();
+        ci = next_ci;
+        mis = next_mis;
+    }
+    const double s = block_sum(nrm);
+    if (threadIdx.x == 0) atomicAdd(&S.ctrl->dt2_sq, 4.0 * s);
+}
+
 // --------------------------------------------------------- T1 update ----
 // R1 = f_ph + F2 + f_pp t1 - t1 Q/2 + t1 X_hh(T1 eq); Jacobi + mixing;
 // energy sum_ai f_ai t1'_ai (coupled_cluster.py:342-414, 265-286).
@@ -687,6 +1015,16 @@ int64_t smem_limit() {
     return g_smem_limit;
 }
 
+constexpr int kLatThreadsF32 = 256;   // 5 groups of 49 hole pairs, 2 blocks per SM
+constexpr int kLatThreadsF64 = 512;   // 10 groups, 1 block per SM
+
+// The lattice path of the T2 update applies (7 holes per label, diagonal
+// ladders, short f_pp rows) and its shared memory fits.
+bool use_lat(const nlb_struct_problem* P, size_t el) {
+    return P->uniform_nh == 7 && P->diag_ladders && P->max_fpp_offdiag <= kLatNa &&
+           lat_smem(P->max_row, 7, (int64_t)el).total + 1024 <= smem_limit();
+}
+
 int valid(const nlb_struct_problem* P, const nlb_struct_state* S) {
     if (!P || !S || !S->ctrl) return fail(NLB_ERR_ARG, "null problem/state");
     if (P->p <= 0 || P->h <= 0 || P->n_channels < 0) return fail(NLB_ERR_SIZE, "bad p/h/channels");
@@ -710,7 +1048,16 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
             if (P->n_t2 > 0) k_ga<T><<<grid_for(k_ga<T>, P->n_g), kThreads, 0, st>>>(*P, *S);
             break;
         case NLB_STAGE_T2:
-            if (P->n_t2 > 0) {
+            if (P->n_t2 > 0 && use_lat(P, sizeof(T))) {
+                constexpr int nt = sizeof(T) == 4 ? kLatThreadsF32 : kLatThreadsF64;
+                constexpr int minb = sizeof(T) == 4 ? 2 : 1;
+                const int64_t sm = lat_smem(P->max_row, 7, sizeof(T)).total;
+                auto kern = k_t2_lat<T, 7, nt, minb>;
+                const int bps = blocks_per_sm(reinterpret_cast<const void*>(kern), sm, nt);
+                int64_t grid = (int64_t)num_sms() * bps;
+                if (grid > P->n_rows) grid = P->n_rows;
+                kern<<<(unsigned)grid, nt, (size_t)sm, st>>>(*P, *S);
+            } else if (P->n_t2 > 0) {
                 const int64_t sm = smem_bytes(P, sizeof(T) == 8 ? NLB_F64 : NLB_F32);
                 auto kern = P->uniform_nh == 7 ? k_t2_rows<T, 7> : P->uniform_nh == 1 ? k_t2_rows<T, 1>
                                                                                          : k_t2_rows<T, 0>;

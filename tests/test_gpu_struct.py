@@ -137,3 +137,37 @@ def test_nan_input_reports_divergence():
     info = {}
     ccsd_solver(fock, two, eps=1e-12, maxSteps=50, max_diis=0, device=DEV, info=info)
     assert info["status"] == "diverged"
+
+
+def _lattice_engine(L, A, general=False):
+    from nulattice_b200 import structure as S
+    from nulattice_b200.ccsd import StructuredEngine
+    v2, w3 = ham.contact_couplings(-3.0, 1.0)
+    e_ref, fock, two = ham.normal_ordered_hamiltonian(L, ham.closed_shell_holes(L, A), v2, v2, w3, dense=False)
+    plan, why = S.detect(fock, two)
+    assert plan is not None, why
+    eng = StructuredEngine(plan, fock, torch.device(DEV))
+    assert eng.prob.uniform_nh == 7 and eng.prob.diag_ladders and eng.prob.max_fpp_offdiag == 6
+    if general:
+        eng.prob.max_fpp_offdiag = 99   # the one-hole-pair-per-thread lattice kernel no longer applies
+    return eng
+
+
+@pytest.mark.parametrize("L", [3, 4, 5])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 1e-5)])
+def test_lattice_t2_kernel_matches_general_kernel(L, precision, tol):
+    """Seven-hole lattice T2 kernel vs the general row kernel: same steps,
+    DIIS pulses included, on rows of 20, 63 and 118 particles per label."""
+    from nulattice_b200.ccsd import solve_structured
+    out = []
+    for general in (False, True):
+        eng = _lattice_engine(L, 28, general)
+        info = {}
+        e, t1, t2 = solve_structured(eng, eps=0.0, maxSteps=11, max_diis=4, precision=precision,
+                                     mixed_eps=0.0, refine=False, t2_format="compact", info=info)
+        out.append((e, t1.cpu().numpy(), t2.double().cpu().numpy()))
+    (ea, t1a, t2a), (eb, t1b, t2b) = out
+    assert np.abs(t2a).max() > 1e-4
+    assert ea == pytest.approx(eb, rel=tol)
+    np.testing.assert_allclose(t1a, t1b, atol=tol * np.abs(t1b).max())
+    np.testing.assert_allclose(t2a, t2b, atol=tol * np.abs(t2b).max())

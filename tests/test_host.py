@@ -121,4 +121,4 @@ def test_library_exports_declared_symbols():
         assert hasattr(L, s), s
     assert L.nlb_version() >= 1
     assert ctypes.sizeof(_lib.Ctrl) == 1064
-    assert ctypes.sizeof(_lib.StructProblem) == 312
+    assert ctypes.sizeof(_lib.StructProblem) == 320
