@@ -339,9 +339,17 @@ def adjoint_leg(dev):
     info = {}
     E, g2, g3 = A.ccsd_energy_and_gradient(L_BENCH, holes, C2, C3, device=dev, precision="mixed", eps=1e-10,
                                            mixed_eps=1e-8, lambda_tol=1e-8, info=info)
-    info2 = {}
-    E, g2, g3 = A.ccsd_energy_and_gradient(L_BENCH, holes, C2, C3, device=dev, precision="mixed", eps=1e-10,
-                                           mixed_eps=1e-8, lambda_tol=1e-8, info=info2)
+    # timed on the warm engine (buffers allocated, step graphs captured):
+    # forward and Lambda solves measured the same way, median of three
+    runs = []
+    for _ in range(3):
+        info2 = {}
+        E, g2, g3 = A.ccsd_energy_and_gradient(L_BENCH, holes, C2, C3, device=dev, precision="mixed", eps=1e-10,
+                                               mixed_eps=1e-8, lambda_tol=1e-8, info=info2,
+                                               engine=info["engine"])
+        runs.append(info2)
+    runs.sort(key=lambda r: r["t_forward"] + r["t_lambda"])
+    info2 = runs[1]
 
     def etot(c2, c3):
         v, w = ham.contact_couplings(c2, c3)
@@ -359,8 +367,10 @@ def adjoint_leg(dev):
             "t_forward_s": info2["t_forward"], "t_lambda_s": info2["t_lambda"],
             "lambda_over_forward": info2["t_lambda"] / info2["t_forward"],
             "lambda_iters": info2["lambda_iters"], "forward_iters": info2["iterations"],
-            "forward": "mixed precision + FP64 finish to eps 1e-10", "lambda": "FP64, relative step 1e-8",
-            "units": "energy hbar^2/(2 M a^2), couplings hbar^2/(M a^2); wall time incl. host syncs"}
+            "lambda_iters_fp32": info2.get("lambda_iters_fp32"), "lambda_path": info2.get("lambda_path"),
+            "forward": "mixed precision + FP64 finish to eps 1e-10",
+            "lambda": "FP32 pulsed-DIIS Jacobi to relative step 1e-6, FP64 finish to 1e-8",
+            "units": "energy hbar^2/(2 M a^2), couplings hbar^2/(M a^2); wall time incl. host syncs, warm engine"}
 
 
 def e2e_leg(args, fock, two, dev):

@@ -196,31 +196,50 @@ int nlb_struct_pack_t2(const nlb_struct_problem *prob, const double *t2_dense, v
 
 /* ---------------------------------------------------------------------
  * Adjoint of the structured engine (no counterpart in the reference, which
- * has no gradients): CC Lambda equations at converged amplitudes, FP64.
+ * has no gradients): CC Lambda equations at converged amplitudes.
+ *
+ * Seven holes per label with diagonal ladders (closed-site lattice inputs)
+ * take the lattice path: FP32 or FP64 multipliers (dtype), pulsed DIIS on
+ * the Jacobi iteration.  Other inputs take the general path (FP64 only).
  * --------------------------------------------------------------------- */
 typedef struct {
-    double *lam1[2];    /* [p*h] multipliers of the T1 equation (double-buffered) */
-    double *lam2[2];    /* [n_t2] multipliers of the compact T2 equation */
+    double *lam1[2];    /* [p*h] multipliers of the T1 equation (double-buffered, FP64) */
+    void *lam2[2];      /* [n_t2] multipliers of the compact T2 equation (dtype) */
     const double *t1;   /* converged t1 [p*h] */
-    const double *t2;   /* converged compact t2 [n_t2], FP64 */
+    const void *t2;     /* converged compact t2 [n_t2] (dtype) */
     double *prep;       /* [nlb_struct_prep_len] tables at the converged t1 (filled by init) */
-    double *ga;         /* [n_g] Ga of the converged t2 (filled by init) */
-    double *ha;         /* [n_g] scratch */
+    void *ga;           /* [n_g] Ga of the converged t2 (dtype, filled by init) */
+    void *ha;           /* [n_g] scratch (dtype) */
     double *acc;        /* [nlb_lambda_acc_len] scratch; after a step it holds Y1, U, T */
     nlb_ctrl *ctrl;
+    void *gb;           /* [nlb_lambda_gb_len] Gb of every row of the converged t2 (dtype, lattice path) */
+    double *diis_t1;    /* [max_diis*p*h] DIIS error ring, or NULL without DIIS */
+    void *diis_t2;      /* [max_diis*n_t2] (dtype), or NULL */
+    int32_t dtype;      /* NLB_F32 or NLB_F64 */
+    int32_t reserved;   /* 0 */
 } nlb_lambda_state;
 
+#define NLB_LAMBDA_KEEP 1   /* nlb_lambda_init: start from lam1[0], lam2[0] instead of zero */
+
 int64_t nlb_lambda_acc_len(const nlb_struct_problem *prob);
-/* Zero the multipliers, build the tables at (t1, t2), reset ctrl; tol is the
- * relative step size of the multipliers that ends the iteration. */
+int64_t nlb_lambda_gb_len(const nlb_struct_problem *prob);
+/* 1 when the lattice path applies to prob (FP32 and DIIS available). */
+int32_t nlb_lambda_lattice(const nlb_struct_problem *prob);
+/* Build the tables at (t1, t2), reset ctrl and zero the multipliers (unless
+ * flags has NLB_LAMBDA_KEEP); tol is the relative step size of the
+ * multipliers that ends the iteration, max_diis the DIIS subspace (0: none). */
 int nlb_lambda_init(const nlb_struct_problem *prob, const nlb_lambda_state *st, double tol,
-                    double mixing, int32_t max_steps, nlb_stream_t stream);
+                    double mixing, int32_t max_steps, int32_t max_diis, int32_t flags, nlb_stream_t stream);
 /* One Jacobi step of the Lambda equations; does nothing once ctrl->status is
  * not NLB_RUNNING, so the accumulators keep U = t1^T lam1 and T of the last
- * step that ran. */
+ * step that ran.  With DIIS the step stores its error vector. */
 int nlb_lambda_step(const nlb_struct_problem *prob, const nlb_lambda_state *st, nlb_stream_t stream);
+/* DIIS extrapolation of the multipliers when the last step filled the
+ * subspace (a no-op otherwise); call after every max_diis-th step. */
+int nlb_lambda_diis(const nlb_struct_problem *prob, const nlb_lambda_state *st, int32_t max_diis,
+                    nlb_stream_t stream);
 /* *out = <lam2, (dW + dV) tau> for diagonal derivative ladders
- * dw[hh_ptr_off + hp], dv[pp_ptr_off + ab] (tau = t2 + t1 t1). */
+ * dw[hh_ptr_off + hp], dv[pp_ptr_off + ab] (tau = t2 + t1 t1); FP64 state. */
 int nlb_lambda_coupling(const nlb_struct_problem *prob, const nlb_lambda_state *st, const double *dw,
                         const double *dv, double *out, nlb_stream_t stream);
 

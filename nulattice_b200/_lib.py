@@ -58,7 +58,11 @@ class StructState(ctypes.Structure):
 
 class LambdaState(ctypes.Structure):
     _fields_ = [("lam1", c_void_p * 2), ("lam2", c_void_p * 2)] + [
-        (n, c_void_p) for n in ("t1", "t2", "prep", "ga", "ha", "acc", "ctrl")]
+        (n, c_void_p) for n in ("t1", "t2", "prep", "ga", "ha", "acc", "ctrl", "gb", "diis_t1", "diis_t2")] + [
+        ("dtype", c_int32), ("reserved", c_int32)]
+
+
+NLB_LAMBDA_KEEP = 1
 
 
 class ContractDesc(ctypes.Structure):
@@ -122,12 +126,17 @@ def lib():
     L.nlb_dense_energy_f64.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]
     L.nlb_lambda_acc_len.argtypes = [ctypes.POINTER(StructProblem)]
     L.nlb_lambda_acc_len.restype = c_int64
+    L.nlb_lambda_gb_len.argtypes = [ctypes.POINTER(StructProblem)]
+    L.nlb_lambda_gb_len.restype = c_int64
+    L.nlb_lambda_lattice.argtypes = [ctypes.POINTER(StructProblem)]
+    L.nlb_lambda_lattice.restype = c_int32
     L.nlb_lambda_init.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_double, c_double,
-                                  c_int32, c_void_p]
+                                  c_int32, c_int32, c_int32, c_void_p]
     L.nlb_lambda_step.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_void_p]
+    L.nlb_lambda_diis.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_int32, c_void_p]
     L.nlb_lambda_coupling.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_void_p,
                                       c_void_p, c_void_p, c_void_p]
-    for name in ("nlb_lambda_init", "nlb_lambda_step", "nlb_lambda_coupling"):
+    for name in ("nlb_lambda_init", "nlb_lambda_step", "nlb_lambda_diis", "nlb_lambda_coupling"):
         getattr(L, name).restype = c_int32
     L.nlb_antisym_project_f64.argtypes = [c_void_p, c_int64, c_int64, c_void_p]
     L.nlb_antisym_project_f64.restype = c_int32

@@ -337,8 +337,6 @@ struct LatSmem {
     int64_t row0, row1, gb, rec, dp, off, val, total;
 };
 
-__host__ __device__ inline int64_t lat_round16(int64_t b) { return (b + 15) & ~int64_t(15); }
-
 // Shared-memory layout of k_t2_lat for element size el and NH holes per label.
 __host__ __device__ inline LatSmem lat_smem(int64_t max_row, int nh, int64_t el) {
     const int64_t np2 = max_row / (nh * nh);
@@ -354,43 +352,6 @@ __host__ __device__ inline LatSmem lat_smem(int64_t max_row, int nh, int64_t el)
     s.total = s.val + lat_round16(el * np2 * kLatNb);
     return s;
 }
-
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-
-template <int N>
-__device__ __forceinline__ void cp_async_el(void* dst, const void* src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(N) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Eight consecutive shared-memory values (16-byte aligned) with vector loads.
-__device__ __forceinline__ void lds8(const float* p, float (&v)[8]) {
-    const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-}
-__device__ __forceinline__ void lds8(const double* p, double (&v)[8]) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const double2 a = reinterpret_cast<const double2*>(p)[k];
-        v[2 * k] = a.x; v[2 * k + 1] = a.y;
-    }
-}
-__device__ __forceinline__ void lds8(const int32_t* p, int (&v)[8]) {
-    const int4 a = reinterpret_cast<const int4*>(p)[0], b = reinterpret_cast<const int4*>(p)[1];
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-}
-
-// Jacobi quotient R / D.  FP32 amplitudes: the approximate reciprocal (the
-// denominators only set the step length, the fixed point R = 0 does not
-// depend on them); FP64: IEEE division.
-__device__ __forceinline__ float lat_div(float r, float d) { return __fdividef(r, d); }
-__device__ __forceinline__ double lat_div(double r, double d) { return r / d; }
 
 // Queue the asynchronous copy of the row starting at `src` (rowlen elements)
 // into the buffer `dst`; returns the element shift that makes the 16-byte

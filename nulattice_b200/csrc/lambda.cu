@@ -1,4 +1,4 @@
-// Adjoint (CC Lambda) kernels of the structured engine, FP64, sm_100a.
+// Adjoint (CC Lambda) kernels of the structured engine, sm_100a.
 //
 // At converged amplitudes (t1, t2) the coupling derivative of the CCSD energy
 // is dE/dc = dE_ref/dc + <lam1, R1(t; dH)> + <Lam, R2(t; dH)>, where the
@@ -10,7 +10,18 @@
 // transposed terms below mirror the forward kernels of ccsd_struct.cu one by
 // one (stencils and ladders are symmetric, the X_hh mixing is transposed, the
 // rank-h parts swap the roles of t1 and f_ph).  The equations are iterated
-// with the forward Jacobi denominators and mixing.
+// with the forward Jacobi denominators and mixing, optionally with the same
+// pulsed DIIS as the forward solve (the Lambda equations are linear, so the
+// extrapolation pays off quickly).
+//
+// Two paths:
+// * general (any hole counts, FP64): one block per row task, every
+//   contraction of the row in shared memory (k_l_rows);
+// * lattice (seven holes per label, diagonal ladders, short f_pp rows; FP32
+//   or FP64): a column pass over the multipliers (k_l_cols: Ha, the Z1
+//   contributions of the particles b' and the hole-hole contractions T) and
+//   a row pass laid out like the forward k_t2_lat (k_l_lat: Z2, the Jacobi
+//   update and the Z1 contributions of the particles a').
 
 #include <cuda_runtime.h>
 #include <math.h>
@@ -57,47 +68,28 @@ __host__ __device__ inline LView lview(double* acc, const nlb_struct_problem& P)
     return v;
 }
 
+// f_ph[P_g[a'], H_g[k']] for entry q of the label-ordered t1 tables.
+__device__ __forceinline__ double fc_entry(const nlb_struct_problem& P, int64_t q) {
+    const int g = find_label(P.t1c_base, P.n_labels, q);
+    const int nh = P.h_base[g + 1] - P.h_base[g];
+    const int loc = (int)(q - P.t1c_base[g]);
+    const int ap = loc / nh, kq = loc - ap * nh;
+    return P.f_ph[(int64_t)P.p_ord[P.p_base[g] + ap] * P.h + P.h_ord[P.h_base[g] + kq]];
+}
+
+// =================================================== general path (FP64) ==
+
 // Tables at the converged amplitudes: prep, Ga, and the per-label f_ph copy.
 __global__ void k_l_setup(nlb_struct_problem P, nlb_lambda_state S) {
     const int64_t nprep = (int64_t)P.h * P.h + 2 * (int64_t)P.p + P.n_t1c + P.n_xc + P.h;
     const LView V = lview(S.acc, P);
+    const double* t2 = static_cast<const double*>(S.t2);
+    double* ga = static_cast<double*>(S.ga);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nprep + P.n_g + P.n_t1c; u += stride) {
-        if (u < nprep) {
-            prep_body(P, S.t1, S.prep, u);
-        } else if (u < nprep + P.n_g) {
-            S.ga[u - nprep] = ga_element(P, S.t2, u - nprep);
-        } else {
-            const int64_t q = u - nprep - P.n_g;
-            const int g = find_label(P.t1c_base, P.n_labels, q);
-            const int nh = P.h_base[g + 1] - P.h_base[g];
-            const int loc = (int)(q - P.t1c_base[g]);
-            const int ap = loc / nh, kq = loc - ap * nh;
-            V.fc[q] = P.f_ph[(int64_t)P.p_ord[P.p_base[g] + ap] * P.h + P.h_ord[P.h_base[g] + kq]];
-        }
-    }
-}
-
-// U = t1^T lam1 and zeroed accumulators.
-__global__ void k_l_prep(nlb_struct_problem P, nlb_lambda_state S) {
-    const nlb_ctrl* c = S.ctrl;
-    if (c->status != NLB_RUNNING) return;
-    const double* l1 = S.lam1[c->parity];
-    const LView V = lview(S.acc, P);
-    const int h = P.h, p = P.p;
-    const int64_t hh = (int64_t)h * h, ph = (int64_t)p * h;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < 2 * hh + ph; u += stride) {
-        if (u < hh) {
-            const int k = (int)(u / h), m = (int)(u % h);
-            double s = 0.0;
-            for (int a = 0; a < p; ++a) s += S.t1[(int64_t)a * h + k] * l1[(int64_t)a * h + m];
-            V.U[u] = s;
-        } else if (u < 2 * hh) {
-            V.T[u - hh] = 0.0;
-        } else {
-            V.Y1[u - 2 * hh] = 0.0;
-        }
+        if (u < nprep) prep_body(P, S.t1, S.prep, u);
+        else if (u < nprep + P.n_g) ga[u - nprep] = ga_element(P, t2, u - nprep);
+        else V.fc[u - nprep - P.n_g] = fc_entry(P, u - nprep - P.n_g);
     }
 }
 
@@ -105,7 +97,8 @@ __global__ void k_l_prep(nlb_struct_problem P, nlb_lambda_state S) {
 __global__ void k_l_ha(nlb_struct_problem P, nlb_lambda_state S) {
     const nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
-    const double* Lm = S.lam2[c->parity];
+    const double* Lm = static_cast<const double*>(S.lam2[c->parity]);
+    double* ha = static_cast<double*>(S.ha);
     const PrepView PV = prep_view(S.prep, P);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_g; u += stride) {
@@ -118,7 +111,7 @@ __global__ void k_l_ha(nlb_struct_problem P, nlb_lambda_state S) {
         const double* col = Lm + ch.offset + e;
         double acc = 0.0;
         for (int ap = 0; ap < ch.np1; ++ap) acc += t1a[ap * ch.nh1] * col[(int64_t)ap * rowlen];
-        S.ha[u] = acc;
+        ha[u] = acc;
     }
 }
 
@@ -129,10 +122,14 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
     const nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
     const int par = c->parity;
-    const double* __restrict__ Lm = S.lam2[par];
-    double* __restrict__ Lo = S.lam2[par ^ 1];
+    const double* __restrict__ Lm = static_cast<const double*>(S.lam2[par]);
+    double* __restrict__ Lo = static_cast<double*>(S.lam2[par ^ 1]);
     const double* __restrict__ l1 = S.lam1[par];
-    const double* __restrict__ B = S.t2;
+    const double* __restrict__ B = static_cast<const double*>(S.t2);
+    const double* __restrict__ ga = static_cast<const double*>(S.ga);
+    const double* __restrict__ ha = static_cast<const double*>(S.ha);
+    double* E2 = (S.diis_t2 != nullptr && c->max_diis > 0 && c->diis_count < c->max_diis)
+                     ? static_cast<double*>(S.diis_t2) + (int64_t)c->diis_count * P.n_t2 : nullptr;
     const PrepView PV = prep_view(S.prep, P);
     const LView V = lview(S.acc, P);
     const double m = c->mixing;
@@ -202,7 +199,7 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
                 Z += P.fpp_val[q] * ((col == ap) ? x : Lm[ch.offset + (int64_t)col * rowlen + e]);
             }
             for (int k = 0; k < nh2; ++k) Z -= f2c[bp * nh2 + k] * shb[k * nhp + hp];
-            for (int k = 0; k < nh1; ++k) Z -= sf1a[k] * S.ha[ch.ga_off + (int64_t)k * rowlen + e];
+            for (int k = 0; k < nh1; ++k) Z -= sf1a[k] * ha[ch.ga_off + (int64_t)k * rowlen + e];
             for (int k = 0; k < nh1; ++k) Z += sx1[ip * nh1 + k] * lrow[bp * nhp + k * nh2 + jp];
             for (int k = 0; k < nh2; ++k) Z += sx2[jp * nh2 + k] * lrow[bp * nhp + ip * nh2 + k];
             const int ab = ap * np2 + bp;
@@ -213,6 +210,7 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
             const double D = -((da + PV.dpc[ch.pb2 + bp]) + (PV.dhc[ch.hb1 + ip] + PV.dhc[ch.hb2 + jp]));
             const double out = x + (1.0 - m) * Z / D;
             Lo[rbase + e] = out;
+            if (E2) E2[rbase + e] = out - x;
             dnrm += (out - x) * (out - x);
             lnrm += out * out;
         }
@@ -252,7 +250,7 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
         for (int q = 0; q < 2 * nh1; ++q) {
             double part = 0.0;
             if (q < nh1) {
-                for (int e = tid; e < rowlen; e += nt) part += lrow[e] * S.ga[ch.ga_off + (int64_t)q * rowlen + e];
+                for (int e = tid; e < rowlen; e += nt) part += lrow[e] * ga[ch.ga_off + (int64_t)q * rowlen + e];
                 part = -part;
             } else {
                 const int iq = q - nh1;
@@ -276,6 +274,39 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
     }
 }
 
+// ========================================================== both paths ==
+
+// U = t1^T lam1 (one warp per hole pair of one label; pairs of different
+// labels vanish) and zeroed accumulators Y1, T.
+__global__ void k_l_u(nlb_struct_problem P, nlb_lambda_state S) {
+    const nlb_ctrl* c = S.ctrl;
+    if (c->status != NLB_RUNNING) return;
+    const double* l1 = S.lam1[c->parity];
+    const LView V = lview(S.acc, P);
+    const int h = P.h;
+    const int64_t hh = (int64_t)h * h, ph = (int64_t)P.p * h;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = warp; u < hh; u += nwarps) {
+        const int k = (int)(u / h), mm = (int)(u % h);
+        const int g = P.h_label[k];
+        double s = 0.0;
+        if (P.h_label[mm] == g)
+            for (int i = P.p_base[g] + lane; i < P.p_base[g + 1]; i += 32) {
+                const int64_t a = P.p_ord[i];
+                s += S.t1[a * h + k] * l1[a * h + mm];
+            }
+        s = warp_sum(s);
+        if (lane == 0) V.U[u] = s;
+    }
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < hh + ph; u += stride) {
+        if (u < hh) V.T[u] = 0.0;
+        else V.Y1[u - hh] = 0.0;
+    }
+}
+
 // Z1 and the Jacobi update of lam1.
 __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
     nlb_ctrl* c = S.ctrl;
@@ -287,6 +318,8 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
     const LView V = lview(S.acc, P);
     const int h = P.h, p = P.p;
     const double m = c->mixing;
+    double* E1 = (S.diis_t1 != nullptr && c->max_diis > 0 && c->diis_count < c->max_diis)
+                     ? S.diis_t1 + (int64_t)c->diis_count * p * h : nullptr;
     double dn = 0.0, ln = 0.0;
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (int64_t)p * h;
          idx += (int64_t)gridDim.x * blockDim.x) {
@@ -294,6 +327,7 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
         const int g = P.p_label[x];
         if (P.h_label[mm] != g) {
             lo[idx] = 0.0;
+            if (E1) E1[idx] = 0.0;
             continue;
         }
         double Z = P.f_ph[idx] + V.Y1[idx];
@@ -312,6 +346,7 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
         const double D1 = -(PV.dXp1[x] + PV.Xh1[(int64_t)mm * h + mm]);
         const double out = l1[idx] + (1.0 - m) * Z / D1;
         lo[idx] = out;
+        if (E1) E1[idx] = out - l1[idx];
         dn += (out - l1[idx]) * (out - l1[idx]);
         ln += out * out;
     }
@@ -323,34 +358,50 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
     }
 }
 
-// convergence on the relative step of the multipliers
+// Convergence on the relative step of the multipliers; DIIS bookkeeping as
+// in the forward k_finish (a pulse when max_diis error vectors are stored).
 __global__ void k_l_finish(nlb_ctrl* c) {
     if (threadIdx.x != 0 || blockIdx.x != 0 || c->status != NLB_RUNNING) return;
     c->iter += 1;
     c->parity ^= 1;
+    c->diis_pulse = 0;
     const double step = sqrt(c->dt1_sq + c->dt2_sq), size = sqrt(c->e_acc);
     c->e_last = step;
-    if (step < c->eps * fmax(1.0, size)) c->status = NLB_CONVERGED;
-    else if (!(step == step) || step > 1e12) c->status = NLB_DIVERGED;
-    else if (c->iter >= c->max_steps) c->status = NLB_MAX_ITER;
+    if (step < c->eps * fmax(1.0, size)) {
+        c->status = NLB_CONVERGED;
+    } else if (!(step == step) || step > 1e12) {
+        c->status = NLB_DIVERGED;
+    } else {
+        if (c->max_diis > 0) {
+            c->diis_count += 1;
+            if (c->diis_count == c->max_diis) {
+                c->diis_pulse = 1;
+                for (int k = 0; k < 121; ++k) c->gram[k] = 0.0;
+            }
+        }
+        if (c->iter >= c->max_steps) c->status = NLB_MAX_ITER;
+    }
     c->dt1_sq = 0.0;
     c->dt2_sq = 0.0;
     c->e_acc = 0.0;
 }
 
-__global__ void k_l_init(nlb_ctrl* c, double tol, double mixing, int max_steps) {
+__global__ void k_l_init(nlb_ctrl* c, double tol, double mixing, int max_steps, int max_diis) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     c->e_acc = 0.0; c->dt1_sq = 0.0; c->dt2_sq = 0.0; c->e_prev = 0.0; c->e_last = 0.0;
     c->eps = tol; c->mixing = mixing;
     c->parity = 0; c->iter = 0; c->status = max_steps > 0 ? NLB_RUNNING : NLB_MAX_ITER; c->max_steps = max_steps;
-    c->criterion = 0; c->max_diis = 0; c->diis_count = 0; c->diis_pulse = 0; c->diis_applied = 0; c->ccs = 0;
+    c->criterion = NLB_CRIT_SOA; c->max_diis = max_diis; c->diis_count = 0; c->diis_pulse = 0;
+    c->diis_applied = 0; c->ccs = 0;
+    for (int k = 0; k < 121; ++k) c->gram[k] = 0.0;
 }
 
 // <Lam, (dW + dV) tau> over the compact layout for a derivative Hamiltonian
 // whose ladders are diagonal: dw[hh_ptr_off + hp], dv[pp_ptr_off + ab].
 __global__ void k_l_coupling(nlb_struct_problem P, nlb_lambda_state S, const double* dw, const double* dv,
                              double* out) {
-    const double* Lm = S.lam2[S.ctrl->parity];
+    const double* Lm = static_cast<const double*>(S.lam2[S.ctrl->parity]);
+    const double* t2 = static_cast<const double*>(S.t2);
     const PrepView PV = prep_view(S.prep, P);
     double acc = 0.0;
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_t2; u += (int64_t)gridDim.x * blockDim.x) {
@@ -362,14 +413,446 @@ __global__ void k_l_coupling(nlb_struct_problem P, nlb_lambda_state S, const dou
         const int ab = (int)(loc / nhp);
         const int ap = ab / ch.np2, bp = ab - ap * ch.np2;
         const int ip = hp / ch.nh2, jp = hp - ip * ch.nh2;
-        const double tau = S.t2[u] + PV.t1c[P.t1c_base[ch.g1] + ap * ch.nh1 + ip] *
-                                         PV.t1c[P.t1c_base[ch.g2] + bp * ch.nh2 + jp];
+        const double tau = t2[u] + PV.t1c[P.t1c_base[ch.g1] + ap * ch.nh1 + ip] *
+                                       PV.t1c[P.t1c_base[ch.g2] + bp * ch.nh2 + jp];
         acc += Lm[u] * (dw[ch.hh_ptr_off + hp] + dv[ch.pp_ptr_off + ab]) * tau;
     }
     const double s = block_sum(acc);
     if (threadIdx.x == 0) atomicAdd(out, s);
 }
 
+// ======================================================== lattice path ==
+constexpr int kLH = 7;                 // holes per label on the lattice path
+constexpr int kLHP = kLH * kLH;
+constexpr int kLNa = 6;                // off-diagonal f_pp entries of a' in registers
+constexpr int kLNb = 8;                // staged f_pp slots of b' (at most 7 used)
+constexpr int kLRec = 24;              // record of b': f_ph[7], flag | lam1[7], pp ladder | t1[7], denominator
+
+// Tables at the converged amplitudes: prep, f_ph per label, Ga and the Gb of
+// every row, both in the multipliers' type.
+template <typename T>
+__global__ void k_l_setup_lat(nlb_struct_problem P, nlb_lambda_state S) {
+    const int64_t nprep = (int64_t)P.h * P.h + 2 * (int64_t)P.p + P.n_t1c + P.n_xc + P.h;
+    const int64_t n_gb = P.n_rows * kLH * kLHP;
+    const LView V = lview(S.acc, P);
+    const T* t2 = static_cast<const T*>(S.t2);
+    T* ga = static_cast<T*>(S.ga);
+    T* gb = static_cast<T*>(S.gb);
+    const int64_t total = nprep + P.n_g + P.n_t1c + n_gb;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += stride) {
+        if (u < nprep) {
+            prep_body(P, S.t1, S.prep, u);
+        } else if (u < nprep + P.n_g) {
+            ga[u - nprep] = ga_element(P, t2, u - nprep);
+        } else if (u < nprep + P.n_g + P.n_t1c) {
+            V.fc[u - nprep - P.n_g] = fc_entry(P, u - nprep - P.n_g);
+        } else {
+            // Gb[row][k'][hp] = sum_c f_ck B[a'][c'][hp], holes k of label g2
+            const int64_t v = u - nprep - P.n_g - P.n_t1c;
+            const int64_t task = v / (kLH * kLHP);
+            const int rem = (int)(v - task * (kLH * kLHP));
+            const int kq = rem / kLHP, hp = rem - kq * kLHP;
+            const int ci = find_seg(P.row_end, P.n_channels, task);
+            const nlb_channel ch = P.chan[ci];
+            const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
+            const int64_t rowlen = (int64_t)ch.np2 * kLHP;
+            const T* Brow = t2 + ch.offset + ap * rowlen;
+            const int row = ch.hb2 + kq;
+            T acc = T(0);
+            for (int q = P.fph_ptr[row]; q < P.fph_ptr[row + 1]; ++q)
+                acc += (T)P.fph_val[q] * Brow[P.fph_col[q] * kLHP + hp];
+            gb[v] = acc;
+        }
+    }
+}
+
+// Column pass over the multipliers Lam (current parity).  A block owns NB
+// consecutive b' of one channel (a group of NH^2 threads per b', a thread per
+// hole pair) and a chunk of the rows a'; per row it accumulates
+//   Ha[k'][b'][hp]  += t1[a', k'] Lam[a'][b'][hp]                       (k' in H_g1)
+//   Y1[b', k']      += Lam[a'][b'][(i', k')] (v_hh + v_pp) t1[a', i'] - Lam[a'][b'][hp] Gb[a'][k'][hp]
+//   T[k', i'] (g1)  += Lam[a'][b'][i', j'] B[a'][b'][k', j']
+//   T[k', j'] (g2)  += Lam[a'][b'][i', j'] B[a'][b'][i', k']
+// and adds its partial sums with atomics (Ha is zeroed before the pass).
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lambda_state S, int nchunk) {
+    constexpr int NB = NT / kLHP;
+    __shared__ double sv[NT][kLH + 1];    // per-thread partial sums, one kind at a time
+    const nlb_ctrl* c = S.ctrl;
+    if (c->status != NLB_RUNNING) return;
+    const T* __restrict__ Lm = static_cast<const T*>(S.lam2[c->parity]);
+    const T* __restrict__ B = static_cast<const T*>(S.t2);
+    const T* __restrict__ gb = static_cast<const T*>(S.gb);
+    T* __restrict__ ha = static_cast<T*>(S.ha);
+    const PrepView PV = prep_view(S.prep, P);
+    const LView V = lview(S.acc, P);
+    const int tid = threadIdx.x;
+    const int grp = tid / kLHP, hp = tid - grp * kLHP;
+    const int ip = hp / kLH, jp = hp - ip * kLH;
+    // work item -> (channel, b' block, row chunk)
+    int64_t item = blockIdx.x;
+    int ci = 0;
+    for (; ci < P.n_channels; ++ci) {
+        const int64_t nit = (int64_t)((P.chan[ci].np2 + NB - 1) / NB) * nchunk;
+        if (item < nit) break;
+        item -= nit;
+    }
+    if (ci >= P.n_channels) return;   // uniform over the block
+    const nlb_channel ch = P.chan[ci];
+    const int bb = (int)(item / nchunk), chunk = (int)(item - (int64_t)bb * nchunk);
+    const int a0 = (int)((int64_t)chunk * ch.np1 / nchunk), a1 = (int)((int64_t)(chunk + 1) * ch.np1 / nchunk);
+    const int bp = bb * NB + grp;
+    const bool act = grp < NB && bp < ch.np2;
+    const int rowlen = ch.np2 * kLHP;
+    T hak[kLH], ys[kLH], tt1[kLH], tt2[kLH];
+    T ylt = T(0);
+#pragma unroll
+    for (int k = 0; k < kLH; ++k) { hak[k] = T(0); ys[k] = T(0); tt1[k] = T(0); tt2[k] = T(0); }
+    const int64_t col = (int64_t)bp * kLHP + hp;   // element offset of (b', hp) in a row
+    if (act) {
+        const int32_t* hptr = P.hh_ptr + ch.hh_ptr_off;
+        const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off + bp;
+        const double* pval = P.pp_val + ch.pp_col_off;
+        const T shh = (hptr[hp + 1] > hptr[hp]) ? (T)P.hh_val[ch.hh_col_off + hptr[hp]] : T(0);
+        const double* t1a = PV.t1c + P.t1c_base[ch.g1];
+        const T* gbr = gb + (ci ? P.row_end[ci - 1] : 0) * (int64_t)(kLH * kLHP) + hp;
+        const T* Lc = Lm + ch.offset + col;
+        const T* Bb = B + ch.offset + (int64_t)bp * kLHP;   // block (a', b') of t2 at + a' rowlen
+        // no barrier in the loop: every operand is an independent load (the
+        // t2 block values come from L1 after the first touch)
+        for (int ap = a0; ap < a1; ++ap) {
+            const int64_t ro = (int64_t)ap * rowlen;
+            const T x = Lc[ro];
+            const T* blk = Bb + ro;
+            T bc[kLH], br[kLH], g[kLH], ta[kLH];
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) {
+                bc[k] = __ldg(blk + k * kLH + jp);
+                br[k] = __ldg(blk + ip * kLH + k);
+                g[k] = __ldg(gbr + (int64_t)ap * (kLH * kLHP) + k * kLHP);
+                ta[k] = (T)__ldg(t1a + ap * kLH + k);
+            }
+            const int ab = ap * ch.np2;
+            const int q0 = __ldg(pptr + ab), q1 = __ldg(pptr + ab + 1);
+            const T cpp = (q1 > q0) ? (T)__ldg(pval + q0) : T(0);
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) {
+                hak[k] += ta[k] * x;
+                ys[k] += x * g[k];
+                tt1[k] += x * bc[k];
+                tt2[k] += x * br[k];
+            }
+            ylt += x * (shh + cpp) * ta[ip];
+        }
+#pragma unroll
+        for (int k = 0; k < kLH; ++k) atomicAdd(&ha[ch.ga_off + (int64_t)k * rowlen + col], hak[k]);
+    }
+    const int h = P.h;
+    // Y1[b', k'] = sum over the group's hole pairs of -ys[k'] + (k' == j') ylt
+#pragma unroll
+    for (int k = 0; k < kLH; ++k) sv[tid][k] = act ? (double)(-ys[k]) + (k == jp ? (double)ylt : 0.0) : 0.0;
+    __syncthreads();
+    for (int w = tid; w < NB * kLH; w += NT) {
+        const int g2 = w / kLH, k = w % kLH;
+        const int b2 = bb * NB + g2;
+        if (b2 < ch.np2) {
+            double s = 0.0;
+            for (int q = 0; q < kLHP; ++q) s += sv[g2 * kLHP + q][k];
+            atomicAdd(&V.Y1[(int64_t)P.p_ord[ch.pb2 + b2] * h + P.h_ord[ch.hb2 + k]], s);
+        }
+    }
+    __syncthreads();
+    // T[k', i'] (g1) = sum over threads with that i'; then T[k', j'] (g2) likewise
+    for (int side = 0; side < 2; ++side) {
+#pragma unroll
+        for (int k = 0; k < kLH; ++k) sv[tid][k] = act ? (double)(side ? tt2[k] : tt1[k]) : 0.0;
+        __syncthreads();
+        for (int w = tid; w < kLHP; w += NT) {
+            const int k = w / kLH, i = w % kLH;
+            double s = 0.0;
+            for (int g2 = 0; g2 < NB; ++g2)
+                for (int o = 0; o < kLH; ++o) s += sv[g2 * kLHP + (side ? o * kLH + i : i * kLH + o)][k];
+            const int hb = side ? ch.hb2 : ch.hb1;
+            atomicAdd(&V.T[(int64_t)P.h_ord[hb + k] * h + P.h_ord[hb + i]], s);
+        }
+        __syncthreads();
+    }
+}
+
+// Shared-memory layout of k_l_lat for element size el and nb hole-pair groups.
+struct LLat {
+    int64_t row, hbp, rec, off, val, total;
+};
+
+__host__ __device__ inline LLat llat_smem(int64_t max_row, int nb, int64_t el) {
+    const int64_t np2 = max_row / kLHP;
+    LLat s;
+    s.row = 0;
+    s.hbp = lat_round16(el * (max_row + 16 / el + 4));
+    s.rec = s.hbp + lat_round16(el * nb * kLH * kLHP);
+    s.off = s.rec + lat_round16(el * np2 * kLRec);
+    s.val = s.off + lat_round16(4 * np2 * kLNb);
+    s.total = s.val + lat_round16(el * np2 * kLNb);
+    return s;
+}
+
+// Row pass (after k_l_cols of the same step): Z2 of row a' and its Jacobi
+// update, and the row's Z1 contributions of particle a'
+//   Y1[a', k'] += -sum_e Lam[a'][e] Ga[k'][e] + sum_{b', j'} Lam[a'][b'][(k', j')] (v_hh + v_pp) t1[b', j'],
+// laid out like the forward k_t2_lat: a thread keeps one hole pair for the
+// whole row, the row sits in shared memory, the terms along a come from L2.
+template <typename T, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_lambda_state S) {
+    constexpr int NB = NT / kLHP;
+    constexpr int VEC = 16 / (int)sizeof(T);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double sred[NT / 32][kLH];
+    const nlb_ctrl* c = S.ctrl;
+    if (c->status != NLB_RUNNING) return;
+    const int par = c->parity;
+    const T* __restrict__ Lm = static_cast<const T*>(S.lam2[par]);
+    T* __restrict__ Lo = static_cast<T*>(S.lam2[par ^ 1]);
+    const double* __restrict__ l1 = S.lam1[par];
+    const T* __restrict__ Ga = static_cast<const T*>(S.ga);
+    const T* __restrict__ Ha = static_cast<const T*>(S.ha);
+    T* E2 = (S.diis_t2 != nullptr && c->max_diis > 0 && c->diis_count < c->max_diis)
+                ? static_cast<T*>(S.diis_t2) + (int64_t)c->diis_count * P.n_t2 : nullptr;
+    const PrepView PV = prep_view(S.prep, P);
+    const LView V = lview(S.acc, P);
+    const T om = (T)(1.0 - c->mixing);
+    const LLat L = llat_smem(P.max_row, NB, sizeof(T));
+    T* srow = reinterpret_cast<T*>(smem_raw + L.row);
+    T* hbp = reinterpret_cast<T*>(smem_raw + L.hbp);       // [NB][k'][hp] partial Hb
+    T* srec = reinterpret_cast<T*>(smem_raw + L.rec);      // [b'][kLRec]
+    int32_t* soff = reinterpret_cast<int32_t*>(smem_raw + L.off);
+    T* sval = reinterpret_cast<T*>(smem_raw + L.val);
+
+    const int tid = threadIdx.x, h = P.h;
+    const bool active = tid < NB * kLHP;
+    const int grp = tid / kLHP, hp = tid - grp * kLHP;
+    const int ip = hp / kLH, jp = hp - ip * kLH;
+    const int lane = tid & 31, wid = tid >> 5;
+    double dnrm = 0.0, lnrm = 0.0;
+    int cur_ci = -1;
+    T x1t[kLH], x2t[kLH], shh = T(0), dh = T(0);
+    const int64_t t0 = (int64_t)blockIdx.x * P.n_rows / gridDim.x;
+    const int64_t t1e = (int64_t)(blockIdx.x + 1) * P.n_rows / gridDim.x;
+    for (int64_t task = t0; task < t1e; ++task) {
+        const int ci = find_seg(P.row_end, P.n_channels, task);
+        const nlb_channel ch = P.chan[ci];
+        const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
+        const int np2 = ch.np2;
+        const int rowlen = np2 * kLHP;
+        const int64_t rbase = ch.offset + (int64_t)ap * rowlen;
+        const int a = P.p_ord[ch.pb1 + ap];
+        // the row, asynchronously (ragged head, 16-byte middle, ragged tail)
+        const T* Lrow = Lm + rbase;
+        const int mis = (int)((reinterpret_cast<uintptr_t>(Lrow) / sizeof(T)) & (VEC - 1));
+        T* sr = srow + mis;
+        {
+            const int head = min((VEC - mis) & (VEC - 1), rowlen);
+            const int nvec = (rowlen - head) / VEC;
+            const int tail0 = head + nvec * VEC;
+            for (int e = tid; e < head; e += NT) cp_async_el<sizeof(T)>(sr + e, Lrow + e);
+            for (int v = tid; v < nvec; v += NT) cp_async16(sr + head + v * VEC, Lrow + head + v * VEC);
+            for (int e = tail0 + tid; e < rowlen; e += NT) cp_async_el<sizeof(T)>(sr + e, Lrow + e);
+            cp_async_commit();
+        }
+        if (ci != cur_ci) {
+            cur_ci = ci;
+            const int x1b = P.xc_base[ch.g1], x2b = P.xc_base[ch.g2];
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) {
+                x1t[k] = (T)PV.xc[x1b + ip * kLH + k];
+                x2t[k] = (T)PV.xc[x2b + jp * kLH + k];
+            }
+            const int32_t* hptr = P.hh_ptr + ch.hh_ptr_off;
+            shh = (hptr[hp + 1] > hptr[hp]) ? (T)P.hh_val[ch.hh_col_off + hptr[hp]] : T(0);
+            dh = (T)(PV.dhc[ch.hb1 + ip] + PV.dhc[ch.hb2 + jp]);
+            const int t1b_b = P.t1c_base[ch.g2];
+            for (int w = tid; w < np2 * kLNb; w += NT) {
+                const int bq = w / kLNb, k = w - bq * kLNb;
+                const int r0 = P.fpp_ptr[ch.pb2 + bq], r1 = P.fpp_ptr[ch.pb2 + bq + 1];
+                soff[w] = ((k < r1 - r0) ? P.fpp_col[r0 + k] : bq) * kLHP;
+                sval[w] = (k < r1 - r0) ? (T)P.fpp_val[r0 + k] : T(0);
+                T* rec = srec + bq * kLRec;
+                if (k < kLH) {
+                    rec[k] = (T)V.fc[t1b_b + bq * kLH + k];
+                    rec[8 + k] = (T)l1[(int64_t)P.p_ord[ch.pb2 + bq] * h + P.h_ord[ch.hb2 + k]];
+                    rec[16 + k] = (T)PV.t1c[t1b_b + bq * kLH + k];
+                } else {
+                    bool nz = false;
+                    for (int kk = 0; kk < kLH; ++kk) nz |= V.fc[t1b_b + bq * kLH + kk] != 0.0;
+                    rec[7] = nz ? T(1) : T(0);   // f_ph row of b' not all zero
+                }
+            }
+        }
+        // per row: f_pp of a' (unused slots point at the row itself with
+        // weight 0), f_ph and lam1 of a', pp ladder entries and denominators
+        const int ra0 = P.fpp_ptr[ch.pb1 + ap], ra1 = P.fpp_ptr[ch.pb1 + ap + 1];
+        T adiag = T(0);
+        int aoff[kLNa];
+        T aval[kLNa];
+        {
+            int q = ra0;
+#pragma unroll
+            for (int s = 0; s < kLNa; ++s) {
+                aoff[s] = ap * rowlen;
+                aval[s] = T(0);
+                for (; q < ra1; ++q) {
+                    const int colq = P.fpp_col[q];
+                    if (colq == ap) { adiag += (T)P.fpp_val[q]; continue; }
+                    aoff[s] = colq * rowlen;
+                    aval[s] = (T)P.fpp_val[q];
+                    ++q;
+                    break;
+                }
+            }
+            for (; q < ra1; ++q)
+                if (P.fpp_col[q] == ap) adiag += (T)P.fpp_val[q];
+        }
+        const int fa_b = P.t1c_base[ch.g1] + ap * kLH;
+        T sf1a[kLH];
+        bool near = false;
+#pragma unroll
+        for (int k = 0; k < kLH; ++k) {
+            sf1a[k] = (T)V.fc[fa_b + k];
+            near |= sf1a[k] != T(0);
+        }
+        const T sf1ai = (T)V.fc[fa_b + ip];
+        const T sl1a = (T)l1[(int64_t)a * h + P.h_ord[ch.hb1 + ip]];
+        const double da = PV.dpc[ch.pb1 + ap];
+        const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off;
+        const double* pval = P.pp_val + ch.pp_col_off;
+        for (int bq = tid; bq < np2; bq += NT) {
+            const int ab = ap * np2 + bq;
+            srec[bq * kLRec + 15] = (pptr[ab + 1] > pptr[ab]) ? (T)pval[pptr[ab]] : T(0);
+            srec[bq * kLRec + 23] = (T)(da + PV.dpc[ch.pb2 + bq]);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        // Hb[k'][hp] = sum_c t1[c, k'] Lam[a'][c][hp] (c in P_g2): group g takes c = g mod NB
+        T hb[kLH];
+        if (active) {
+            T part[kLH];
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) part[k] = T(0);
+            for (int cq = grp; cq < np2; cq += NB) {
+                const T v = sr[cq * kLHP + hp];
+                T t[8];
+                lds8(srec + cq * kLRec + 16, t);
+#pragma unroll
+                for (int k = 0; k < kLH; ++k) part[k] += t[k] * v;
+            }
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) hbp[(grp * kLH + k) * kLHP + hp] = part[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kLH; ++k) hb[k] = T(0);
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) {
+                T s = T(0);
+                for (int g = 0; g < NB; ++g) s += hbp[(g * kLH + k) * kLHP + hp];
+                hb[k] = s;
+            }
+        }
+        T acc_ga[kLH];
+        T acc3 = T(0);
+#pragma unroll
+        for (int k = 0; k < kLH; ++k) acc_ga[k] = T(0);
+        if (active && grp < np2) {
+            const T* __restrict__ gL = Lm + ch.offset + hp;
+            const T* __restrict__ gG = Ga + ch.ga_off + hp;
+            const T* __restrict__ gH = Ha + ch.ga_off + hp;
+            T* __restrict__ Lout = Lo + rbase + hp;
+            T* __restrict__ Eout = E2 ? E2 + rbase + hp : nullptr;
+            const T* s_hp = sr + hp;
+            const T* s_col = sr + jp;            // Lam[a'][b'][k'][j'] at eb + k' NH
+            const T* s_row = sr + ip * kLH;      // Lam[a'][b'][i'][k'] at eb + k'
+            T nrm_d = T(0), nrm_l = T(0);
+            for (int bq = grp; bq < np2; bq += NB) {
+                const int eb = bq * kLHP;
+                T nb[kLNa], gv[kLH];
+#pragma unroll
+                for (int q = 0; q < kLNa; ++q) nb[q] = __ldg(gL + aoff[q] + eb);
+#pragma unroll
+                for (int k = 0; k < kLH; ++k) gv[k] = __ldg(gG + k * rowlen + eb);
+                const T x = s_hp[eb];
+                const T* rec = srec + bq * kLRec;
+                T f2[8], sv[8];
+                int so[8];
+                lds8(rec, f2);
+                lds8(soff + bq * kLNb, so);
+                lds8(sval + bq * kLNb, sv);
+                // f_pp along b
+                T zb = T(0);
+#pragma unroll
+                for (int q = 0; q < kLNb - 1; ++q) zb += sv[q] * s_hp[so[q]];
+                // X_hh along i and j (transposed)
+                T zx = T(0), zy = T(0);
+#pragma unroll
+                for (int k = 0; k < kLH; ++k) {
+                    zx += x1t[k] * s_col[eb + k * kLH];
+                    zy += x2t[k] * s_row[eb + k];
+                }
+                // rank-h parts: -f_ph[b', k'] Hb[k'] and -f_ph[a', k'] Ha[k'] (sparse f_ph)
+                T zh = T(0);
+                if (f2[7] != T(0)) {
+#pragma unroll
+                    for (int k = 0; k < kLH; ++k) zh += f2[k] * hb[k];
+                }
+                if (near) {
+#pragma unroll
+                    for (int k = 0; k < kLH; ++k) zh += sf1a[k] * __ldg(gH + k * rowlen + eb);
+                }
+                // f_pp along a
+                T za = adiag * x;
+#pragma unroll
+                for (int q = 0; q < kLNa; ++q) za += aval[q] * nb[q];
+                const T lad = shh + rec[15];
+                const T f2j = rec[jp], l1bj = rec[8 + jp], t1bj = rec[16 + jp];
+                const T Z = ((za + zb) - zh) + ((zx + zy) + lad * x) + (sl1a * f2j + l1bj * sf1ai);
+                const T D = -(rec[23] + dh);
+                const T out = x + lat_div(om * Z, D);
+                __stcg(Lout + eb, out);
+                const T d = out - x;
+                if (Eout) __stcg(Eout + eb, d);
+                nrm_d += d * d;
+                nrm_l += out * out;
+#pragma unroll
+                for (int k = 0; k < kLH; ++k) acc_ga[k] += x * gv[k];
+                acc3 += x * lad * t1bj;
+            }
+            dnrm += (double)nrm_d;
+            lnrm += (double)nrm_l;
+        }
+        // Y1 of particle a': block sums of -acc_ga[k'] + (k' == i') acc3
+#pragma unroll
+        for (int k = 0; k < kLH; ++k) {
+            double v = -(double)acc_ga[k] + ((active && k == ip) ? (double)acc3 : 0.0);
+            v = warp_sum(v);
+            if (lane == 0) sred[wid][k] = v;
+        }
+        __syncthreads();
+        if (tid < kLH) {
+            double s = 0.0;
+            for (int w = 0; w < NT / 32; ++w) s += sred[w][tid];
+            atomicAdd(&V.Y1[(int64_t)a * h + P.h_ord[ch.hb1 + tid]], s);
+        }
+        __syncthreads();
+    }
+    const double s1 = block_sum(dnrm);
+    const double s2 = block_sum(lnrm);
+    if (tid == 0) {
+        atomicAdd(&S.ctrl->dt2_sq, 4.0 * s1);
+        atomicAdd(&S.ctrl->e_acc, 4.0 * s2);
+    }
+}
+
+// =============================================================== host ==
 int num_sms_l() {
     static int n = 0;
     if (n == 0) {
@@ -379,6 +862,17 @@ int num_sms_l() {
         if (n <= 0) n = 148;
     }
     return n;
+}
+
+int optin_smem() {
+    static int v = 0;
+    if (v == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (v <= 0) v = 227 * 1024;
+    }
+    return v;
 }
 
 int grid_l(int64_t work) {
@@ -392,6 +886,71 @@ int64_t l_smem(const nlb_struct_problem* P) {
     return 8 * (2 * (int64_t)P->max_row + 2 * mh * mh * mh + 3 * mh * mh + 3 * mh);
 }
 
+constexpr int kLatThreads = 256;            // 5 hole-pair groups per block
+constexpr int kColThreads = 256;
+
+bool lattice(const nlb_struct_problem* P) {
+    if (P->uniform_nh != kLH || !P->diag_ladders || P->max_fpp_offdiag > kLNa || P->n_t2 <= 0) return false;
+    return llat_smem(P->max_row, kLatThreads / kLHP, 8).total + 1024 <= optin_smem();
+}
+
+int64_t gb_len(const nlb_struct_problem* P) { return P->n_rows * (int64_t)kLH * kLHP; }
+
+// Blocks per SM of a kernel at a dynamic shared-memory size, queried once.
+int lat_bps(const void* fn, int64_t smem, int threads) {
+    static const void* fns[16] = {};
+    static int64_t sms[16] = {};
+    static int vals[16] = {};
+    for (int k = 0; k < 16; ++k)
+        if (fns[k] == fn && sms[k] == smem) return vals[k];
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, (size_t)smem) != cudaSuccess || bps < 1)
+        bps = 1;
+    for (int k = 0; k < 16; ++k)
+        if (fns[k] == nullptr) { fns[k] = fn; sms[k] = smem; vals[k] = bps; break; }
+    return bps;
+}
+
+// Row chunks of the column pass: about sixteen blocks per SM, at least
+// eight rows per chunk.
+int col_chunks(const nlb_struct_problem* P) {
+    constexpr int NB = kColThreads / kLHP;
+    const int64_t np = P->max_row / kLHP;
+    const int64_t per = (np + NB - 1) / NB * P->n_channels;
+    const int64_t want = (int64_t)num_sms_l() * 16;
+    int64_t n = (want + per - 1) / (per > 0 ? per : 1);
+    if (n > np / 8) n = np / 8;
+    return (int)(n < 1 ? 1 : n);
+}
+
+template <typename T>
+int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_t s) {
+    constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
+    const int64_t hh = (int64_t)P->h * P->h;
+    k_l_u<<<grid_l(32 * hh + (int64_t)P->p * P->h), kThreads, 0, s>>>(*P, *S);
+    cudaMemsetAsync(S->ha, 0, sizeof(T) * (size_t)P->n_g, s);
+    {
+        // every label has the same particle count on the lattice path
+        constexpr int NB = kColThreads / kLHP;
+        const int nchunk = col_chunks(P);
+        const int64_t np2 = P->max_row / kLHP;
+        const int64_t items = (np2 + NB - 1) / NB * nchunk * P->n_channels;
+        k_l_cols<T, kColThreads><<<(unsigned)items, kColThreads, 0, s>>>(*P, *S, nchunk);
+    }
+    {
+        const int64_t sm = llat_smem(P->max_row, kLatThreads / kLHP, sizeof(T)).total;
+        auto kern = k_l_lat<T, kLatThreads, MINB>;
+        const int bps = lat_bps(reinterpret_cast<const void*>(kern), sm, kLatThreads);
+        int64_t grid = (int64_t)num_sms_l() * bps;
+        if (grid > P->n_rows) grid = P->n_rows;
+        kern<<<(unsigned)grid, kLatThreads, (size_t)sm, s>>>(*P, *S);
+    }
+    k_l_t1<<<grid_l((int64_t)P->p * P->h), kThreads, 0, s>>>(*P, *S);
+    k_l_finish<<<1, 32, 0, s>>>(S->ctrl);
+    return lcheck("nlb_lambda_step");
+}
+
 }  // namespace
 
 extern "C" {
@@ -401,49 +960,64 @@ int64_t nlb_lambda_acc_len(const nlb_struct_problem* prob) {
     return (int64_t)prob->p * prob->h + 2 * (int64_t)prob->h * prob->h + prob->n_t1c;
 }
 
+int64_t nlb_lambda_gb_len(const nlb_struct_problem* prob) {
+    if (!prob || !lattice(prob)) return 0;
+    return gb_len(prob);
+}
+
+int32_t nlb_lambda_lattice(const nlb_struct_problem* prob) { return (prob && lattice(prob)) ? 1 : 0; }
+
 int nlb_lambda_init(const nlb_struct_problem* prob, const nlb_lambda_state* st, double tol, double mixing,
-                    int32_t max_steps, nlb_stream_t stream) {
+                    int32_t max_steps, int32_t max_diis, int32_t flags, nlb_stream_t stream) {
     if (!prob || !st || !st->ctrl || !st->t1 || !st->t2 || !st->prep || !st->ga || !st->ha || !st->acc)
         return lfail(NLB_ERR_ARG, "nlb_lambda_init: null argument");
     if (!st->lam1[0] || !st->lam1[1] || !st->lam2[0] || !st->lam2[1])
         return lfail(NLB_ERR_ARG, "nlb_lambda_init: null multiplier buffer");
     if (prob->diag_ladders != 1) return lfail(NLB_ERR_ARG, "nlb_lambda_init: ladders must be diagonal");
-    {
-        int dev = 0, optin = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (st->dtype != NLB_F64 && st->dtype != NLB_F32) return lfail(NLB_ERR_ARG, "nlb_lambda_init: bad dtype");
+    if (max_diis < 0 || max_diis > 10) return lfail(NLB_ERR_ARG, "nlb_lambda_init: max_diis must be in [0, 10]");
+    if (max_diis > 0 && (!st->diis_t1 || !st->diis_t2)) return lfail(NLB_ERR_ARG, "nlb_lambda_init: null DIIS ring");
+    const bool lat = lattice(prob);
+    if (!lat) {
+        if (st->dtype != NLB_F64) return lfail(NLB_ERR_ARG, "nlb_lambda_init: FP32 needs the lattice path");
         cudaFuncAttributes fa;
         cudaFuncGetAttributes(&fa, k_l_rows);
-        if (optin <= 0 || l_smem(prob) + (int64_t)fa.sharedSizeBytes > optin)
+        if (l_smem(prob) + (int64_t)fa.sharedSizeBytes > optin_smem())
             return lfail(NLB_ERR_SIZE, "nlb_lambda_init: a row does not fit in shared memory");
+    } else if (!st->gb) {
+        return lfail(NLB_ERR_ARG, "nlb_lambda_init: null Gb table");
     }
     cudaStream_t s = (cudaStream_t)stream;
-    cudaMemsetAsync(st->lam1[0], 0, sizeof(double) * prob->p * prob->h, s);
+    const size_t el = st->dtype == NLB_F64 ? 8 : 4;
+    if (!(flags & NLB_LAMBDA_KEEP)) {
+        cudaMemsetAsync(st->lam1[0], 0, sizeof(double) * prob->p * prob->h, s);
+        cudaMemsetAsync(st->lam2[0], 0, el * prob->n_t2, s);
+    }
     cudaMemsetAsync(st->lam1[1], 0, sizeof(double) * prob->p * prob->h, s);
-    cudaMemsetAsync(st->lam2[0], 0, sizeof(double) * prob->n_t2, s);
-    cudaMemsetAsync(st->lam2[1], 0, sizeof(double) * prob->n_t2, s);
+    cudaMemsetAsync(st->lam2[1], 0, el * prob->n_t2, s);
     const int64_t nprep = (int64_t)prob->h * prob->h + 2 * (int64_t)prob->p + prob->n_t1c + prob->n_xc + prob->h;
-    k_l_setup<<<grid_l(nprep + prob->n_g + prob->n_t1c), kThreads, 0, s>>>(*prob, *st);
-    k_l_init<<<1, 32, 0, s>>>(st->ctrl, tol, mixing, max_steps);
+    if (lat) {
+        const int64_t tot = nprep + prob->n_g + prob->n_t1c + gb_len(prob);
+        if (st->dtype == NLB_F64) k_l_setup_lat<double><<<grid_l(tot), kThreads, 0, s>>>(*prob, *st);
+        else k_l_setup_lat<float><<<grid_l(tot), kThreads, 0, s>>>(*prob, *st);
+    } else {
+        k_l_setup<<<grid_l(nprep + prob->n_g + prob->n_t1c), kThreads, 0, s>>>(*prob, *st);
+    }
+    k_l_init<<<1, 32, 0, s>>>(st->ctrl, tol, mixing, max_steps, max_diis);
     return lcheck("nlb_lambda_init");
 }
 
 int nlb_lambda_step(const nlb_struct_problem* prob, const nlb_lambda_state* st, nlb_stream_t stream) {
     if (!prob || !st || !st->ctrl) return lfail(NLB_ERR_ARG, "nlb_lambda_step: null argument");
     cudaStream_t s = (cudaStream_t)stream;
+    if (lattice(prob)) return st->dtype == NLB_F64 ? lat_step<double>(prob, st, s) : lat_step<float>(prob, st, s);
+    if (st->dtype != NLB_F64) return lfail(NLB_ERR_ARG, "nlb_lambda_step: FP32 needs the lattice path");
     const int64_t hh = (int64_t)prob->h * prob->h;
-    k_l_prep<<<grid_l(2 * hh + (int64_t)prob->p * prob->h), kThreads, 0, s>>>(*prob, *st);
+    k_l_u<<<grid_l(32 * hh + (int64_t)prob->p * prob->h), kThreads, 0, s>>>(*prob, *st);
     k_l_ha<<<grid_l(prob->n_g), kThreads, 0, s>>>(*prob, *st);
     const int64_t sm = l_smem(prob);
-    static int64_t attr_bytes = 0;
-    if (sm > 48 * 1024 && sm > attr_bytes) {
-        if (cudaFuncSetAttribute(k_l_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-            return lcheck("nlb_lambda_step: shared memory request");
-        attr_bytes = sm;
-    }
-    int bps = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_l_rows, kThreads, (size_t)sm);
-    int64_t grid = (int64_t)num_sms_l() * (bps > 0 ? bps : 1);
+    const int bps = lat_bps(reinterpret_cast<const void*>(k_l_rows), sm, kThreads);
+    int64_t grid = (int64_t)num_sms_l() * bps;
     if (grid > prob->n_rows) grid = prob->n_rows;
     if (grid < 1) grid = 1;
     k_l_rows<<<(unsigned)grid, kThreads, (size_t)sm, s>>>(*prob, *st);
@@ -452,9 +1026,29 @@ int nlb_lambda_step(const nlb_struct_problem* prob, const nlb_lambda_state* st, 
     return lcheck("nlb_lambda_step");
 }
 
+int nlb_lambda_diis(const nlb_struct_problem* prob, const nlb_lambda_state* st, int32_t max_diis,
+                    nlb_stream_t stream) {
+    if (!prob || !st || !st->ctrl) return lfail(NLB_ERR_ARG, "nlb_lambda_diis: null argument");
+    // the forward DIIS kernels on a view of the multipliers
+    nlb_struct_state v = {};
+    v.t1[0] = st->lam1[0];
+    v.t1[1] = st->lam1[1];
+    v.t2[0] = st->lam2[0];
+    v.t2[1] = st->lam2[1];
+    v.g = st->ha;
+    v.f2 = st->acc;
+    v.prep = st->prep;
+    v.ctrl = st->ctrl;
+    v.diis_t1 = st->diis_t1;
+    v.diis_t2 = st->diis_t2;
+    v.dtype = st->dtype;
+    return nlb_struct_diis(prob, &v, max_diis, stream);
+}
+
 int nlb_lambda_coupling(const nlb_struct_problem* prob, const nlb_lambda_state* st, const double* dw,
                         const double* dv, double* out, nlb_stream_t stream) {
     if (!prob || !st || !dw || !dv || !out) return lfail(NLB_ERR_ARG, "nlb_lambda_coupling: null argument");
+    if (st->dtype != NLB_F64) return lfail(NLB_ERR_ARG, "nlb_lambda_coupling: needs the FP64 state");
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemsetAsync(out, 0, sizeof(double), s);
     k_l_coupling<<<grid_l(prob->n_t2), kThreads, 0, s>>>(*prob, *st, dw, dv, out);

@@ -89,3 +89,60 @@ def test_mixed_precision_forward_with_adjoint():
     _, m2, m3 = A.ccsd_energy_and_gradient(L, holes, -3.0, 1.0, device=DEV, precision="mixed")
     assert m2 == pytest.approx(g2, rel=1e-6)
     assert m3 == pytest.approx(g3, rel=1e-6)
+
+
+def _converged(L, A_, general=False):
+    v, w = ham.contact_couplings(-3.0, 1.0)
+    e_ref, fock, two = ham.normal_ordered_hamiltonian(L, ham.closed_shell_holes(L, A_), v, v, w, dense=False)
+    plan, _ = S.detect(fock, two)
+    eng = StructuredEngine(plan, fock, torch.device(DEV))
+    if general:
+        eng.prob.max_fpp_offdiag = 99   # neither lattice kernel applies
+    info = {}
+    e, t1, t2c = solve_structured(eng, eps=1e-14, maxSteps=6000, max_diis=8, t2_format="compact", info=info)
+    assert info["status"] == "converged"
+    return eng, t1, t2c
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_lattice_lambda_steps_match_general_kernels(L):
+    """Three Jacobi steps of the Lambda equations from zero: the lattice
+    kernels (column + row pass) against the general row kernel, FP64 to
+    1e-12 and FP32 to 1e-5, multipliers and the Y1 / U / T accumulators."""
+    from nulattice_b200 import _lib
+    out = {}
+    for kind in ("lattice64", "lattice32", "general"):
+        eng, t1, t2c = _converged(L, 28, general=(kind == "general"))
+        solver = A.LambdaSolver(eng)
+        assert solver.lattice == (kind != "general")
+        code = _lib.NLB_F32 if kind == "lattice32" else _lib.NLB_F64
+        b = solver.buffers(code, 0)
+        b["t1"].copy_(t1.reshape(-1))
+        b["t2"].copy_(t2c.to(b["t2"].dtype))
+        c = solver.run(b, 0.0, 0.5, 3, 0, keep=False)
+        assert c.iter == 3
+        out[kind] = (b["lam1"][c.parity].cpu().numpy(), b["lam2"][c.parity].double().cpu().numpy(),
+                     b["acc"].cpu().numpy())
+    ref = out["general"]
+    for kind, tol in (("lattice64", 1e-12), ("lattice32", 2e-5)):
+        for got, want in zip(out[kind], ref):
+            scale = max(np.abs(want).max(), 1e-30)
+            assert np.abs(got - want).max() <= tol * scale, (kind, np.abs(got - want).max() / scale)
+
+
+def test_lambda_diis_and_mixed_match_jacobi_gradient():
+    """The coupling derivatives do not depend on how the Lambda equations are
+    iterated: Jacobi, pulsed DIIS, and FP32 DIIS with an FP64 finish."""
+    L, A_ = 4, 28
+    eng, t1, t2c = _converged(L, A_)
+    prob = A.lattice_problem(L, ham.closed_shell_holes(L, A_))
+    res = {}
+    for name, kw in (("jacobi", dict(max_diis=0, precision="fp64")), ("diis", dict(max_diis=8, precision="fp64")),
+                     ("mixed", dict(max_diis=8, precision="mixed"))):
+        info = {}
+        res[name] = A.lambda_gradient(eng, t1, t2c, [prob.dv, prob.dw], tol=1e-11, info=info, **kw)
+        assert info["lambda_status"] == "converged" and info["lambda_path"] == "lattice"
+        res[name + "_iters"] = info["lambda_iters"]
+    assert res["diis_iters"] < res["jacobi_iters"]
+    for name in ("diis", "mixed"):
+        np.testing.assert_allclose(res[name], res["jacobi"], rtol=1e-8)
