@@ -244,6 +244,40 @@ int nlb_lambda_coupling(const nlb_struct_problem *prob, const nlb_lambda_state *
                         const double *dv, double *out, nlb_stream_t stream);
 
 /* ---------------------------------------------------------------------
+ * Batched scan (no counterpart in the reference): many structured problems
+ * of uneven size solved, with their coupling derivatives, in ONE CUDA graph
+ * launch.  The graph holds four device-side loops (conditional WHILE nodes):
+ * forward FP32 to mixed_eps, forward FP64 to eps, Lambda FP32 to
+ * lambda_tol_fp32 (lattice instances) and Lambda FP64 to lambda_tol; each
+ * loop body is one branch per instance (chunk steps, DIIS pulses included).
+ * --------------------------------------------------------------------- */
+typedef struct {
+    const nlb_struct_problem *prob;   /* the instance (host struct, device tables) */
+    nlb_struct_state f32, f64;        /* forward buffers (dtype F32 / F64) */
+    nlb_lambda_state l32, l64;        /* Lambda buffers; l32.dtype 0: no FP32 Lambda phase.
+                                         l64.t1/t2 (and l32.t1) must be f64.t1[0]/f64.t2[0];
+                                         l32.t2 receives the converged t2 in FP32 */
+    const double *t1_init;            /* [p*h] start amplitudes (MP2 t1) */
+    double e0;                        /* energy of t1_init */
+    const double *dw[2], *dv[2];      /* diagonal derivative ladders of two couplings (FP64) */
+    double *out;                      /* [8]: E_corr, coupling term 0, coupling term 1, forward status,
+                                         forward iterations, Lambda status, Lambda iterations,
+                                         FP32 forward iterations */
+} nlb_batch_item;
+
+typedef struct {
+    double mixing, mixed_eps, eps, lambda_tol_fp32, lambda_tol;
+    int32_t max_steps, max_diis, lambda_max_steps;
+    int32_t chunk;                    /* steps per loop iteration; a multiple of max_diis */
+} nlb_batch_config;
+
+/* Capture and instantiate the batch graph (buffers stay caller-owned). */
+int nlb_batch_create(const nlb_batch_item *items, int32_t n, const nlb_batch_config *cfg, void **handle);
+/* Launch the whole batch on `stream` (one cudaGraphLaunch). */
+int nlb_batch_launch(void *handle, nlb_stream_t stream);
+int nlb_batch_destroy(void *handle);
+
+/* ---------------------------------------------------------------------
  * General (dense) engine: the full factorised equation set of
  * CCM/coupled_cluster.py:342-545 on dense FP64 tensors in the reference's
  * layouts, for inputs without the closed-site label structure.

@@ -65,6 +65,17 @@ class LambdaState(ctypes.Structure):
 NLB_LAMBDA_KEEP = 1
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [("prob", ctypes.POINTER(StructProblem)), ("f32", StructState), ("f64", StructState),
+                ("l32", LambdaState), ("l64", LambdaState), ("t1_init", c_void_p), ("e0", c_double),
+                ("dw", c_void_p * 2), ("dv", c_void_p * 2), ("out", c_void_p)]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [(n, c_double) for n in ("mixing", "mixed_eps", "eps", "lambda_tol_fp32", "lambda_tol")] + [
+        (n, c_int32) for n in ("max_steps", "max_diis", "lambda_max_steps", "chunk")]
+
+
 class ContractDesc(ctypes.Structure):
     _fields_ = [(n, c_int32) for n in ("nm", "nn", "nk", "nb")] + \
                [(n, c_int64) for n in ("M", "N", "K", "B")] + \
@@ -136,6 +147,12 @@ def lib():
     L.nlb_lambda_diis.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_int32, c_void_p]
     L.nlb_lambda_coupling.argtypes = [ctypes.POINTER(StructProblem), ctypes.POINTER(LambdaState), c_void_p,
                                       c_void_p, c_void_p, c_void_p]
+    L.nlb_batch_create.argtypes = [ctypes.POINTER(BatchItem), c_int32, ctypes.POINTER(BatchConfig),
+                                   ctypes.POINTER(c_void_p)]
+    L.nlb_batch_launch.argtypes = [c_void_p, c_void_p]
+    L.nlb_batch_destroy.argtypes = [c_void_p]
+    for name in ("nlb_batch_create", "nlb_batch_launch", "nlb_batch_destroy"):
+        getattr(L, name).restype = c_int32
     for name in ("nlb_lambda_init", "nlb_lambda_step", "nlb_lambda_diis", "nlb_lambda_coupling"):
         getattr(L, name).restype = c_int32
     L.nlb_antisym_project_f64.argtypes = [c_void_p, c_int64, c_int64, c_void_p]

@@ -937,10 +937,16 @@ struct OccEntry { const void* fn; int64_t smem; int bps; };
 OccEntry g_occ[64];
 int g_nocc = 0;
 
+int64_t smem_limit();
+
 int blocks_per_sm(const void* fn, int64_t smem, int threads = kThreads) {
     for (int k = 0; k < g_nocc; ++k)
         if (g_occ[k].fn == fn && g_occ[k].smem == smem) return g_occ[k].bps;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // raise the limit to the device maximum for every kernel that takes
+    // dynamic shared memory: the 48 KB default counts static shared memory
+    // too, and lowering the limit for a smaller problem would break launches
+    // (and captured graphs) of a larger one
+    if (smem > 0) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem_limit() - 1024));
     int bps = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, (size_t)smem) != cudaSuccess || bps <= 0)
         bps = 1;

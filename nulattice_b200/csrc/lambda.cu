@@ -903,7 +903,11 @@ int lat_bps(const void* fn, int64_t smem, int threads) {
     static int vals[16] = {};
     for (int k = 0; k < 16; ++k)
         if (fns[k] == fn && sms[k] == smem) return vals[k];
-    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // raise the limit to the device maximum for every kernel that takes
+    // dynamic shared memory: the 48 KB default counts static shared memory
+    // too, and lowering the limit for a smaller problem would break launches
+    // (and captured graphs) of a larger one
+    if (smem > 0) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(optin_smem() - 1024));
     int bps = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, (size_t)smem) != cudaSuccess || bps < 1)
         bps = 1;
@@ -946,6 +950,7 @@ int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_
         if (grid > P->n_rows) grid = P->n_rows;
         kern<<<(unsigned)grid, kLatThreads, (size_t)sm, s>>>(*P, *S);
     }
+    if (cudaPeekAtLastError() != cudaSuccess) return lcheck("nlb_lambda_step");
     k_l_t1<<<grid_l((int64_t)P->p * P->h), kThreads, 0, s>>>(*P, *S);
     k_l_finish<<<1, 32, 0, s>>>(S->ctrl);
     return lcheck("nlb_lambda_step");

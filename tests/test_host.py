@@ -122,3 +122,43 @@ def test_library_exports_declared_symbols():
     assert L.nlb_version() >= 1
     assert ctypes.sizeof(_lib.Ctrl) == 1064
     assert ctypes.sizeof(_lib.StructProblem) == 320
+
+
+def test_lambda_and_batch_struct_layouts():
+    from nulattice_b200 import _lib
+    assert ctypes.sizeof(_lib.LambdaState) == 120
+    assert ctypes.sizeof(_lib.BatchItem) == 480
+    assert ctypes.sizeof(_lib.BatchConfig) == 56
+
+
+def test_batch_instances_are_seeded_and_in_range():
+    from nulattice_b200 import batch as B
+    a = B.draw_instances(64, 0)
+    assert a == B.draw_instances(64, 0) and len(a) == 64
+    assert {x[0] for x in a} <= {4, 28} and {x[1] for x in a} <= {4, 5, 6}
+    assert all(-4.0 <= x[2] <= -2.0 and 0.0 <= x[3] <= 2.0 for x in a)
+    # the draw order is A, L, C2, C3 per instance
+    rng = np.random.default_rng(0)
+    first = (int(rng.choice([4, 28])), int(rng.choice([4, 5, 6])), float(rng.uniform(-4, -2)), float(rng.uniform(0, 2)))
+    assert a[0] == first
+
+
+def test_batch_hamiltonian_is_the_builder_output():
+    """H(C2, C3) combined from the (kinetic, contact, three-body) parts equals
+    the direct build, block by block."""
+    from nulattice_b200 import batch as B
+    from nulattice_b200 import hamiltonian as ham
+    from nulattice_b200 import structure as S
+    L, A, C2, C3 = 3, 28, -3.3, 0.7
+    e1, f1, t1 = B.instance_hamiltonian(L, A, C2, C3)
+    v, w = ham.contact_couplings(C2, C3)
+    e2, f2, t2 = ham.normal_ordered_hamiltonian(L, ham.closed_shell_holes(L, A), v, v, w, dense=False)
+    assert e1 == pytest.approx(e2, rel=1e-14)
+    for a, b in zip(f1, f2):
+        np.testing.assert_allclose(a, b, atol=1e-13)
+    for a, b in zip(t1, t2):
+        ia, va = S._coo(a)
+        ib, vb = S._coo(b)
+        oa, ob = np.lexsort(ia.T[::-1]), np.lexsort(ib.T[::-1])
+        np.testing.assert_array_equal(ia[oa], ib[ob])
+        np.testing.assert_allclose(va[oa], vb[ob], atol=1e-13)
