@@ -202,6 +202,10 @@ def main():
     plan, why = S.detect(fock, two)
     assert plan is not None, why
     eng = C.StructuredEngine(plan, fock, dev)
+    # launch shapes of the lattice kernels (timed per variant, cached per GPU and shape)
+    from nulattice_b200 import tune as T
+    tune_info = {}
+    T.tune(eng, info=tune_info)
 
     def solve(precision, t2_events=None, **kw):
         info = {}
@@ -315,6 +319,8 @@ def main():
            "data": "synthetic: lattice Hamiltonian built in-process (no dataset)",
            "config": {"workload": "ccsd_L6_A28_mixed", "L": L_BENCH, "A": A_BENCH, "p": plan.p, "h": plan.h,
                       "C2": C2, "C3": C3, "units": "hbar^2/(M a^2)", "n_t2_compact": n_t2,
+                      "tune": {"word": int(eng.prob.tune), "choice": T.describe(int(eng.prob.tune)),
+                               "measured_us": tune_info.get("us"), "cached": tune_info.get("cached")},
                       "max_diis": 8, "mixed_eps": 1e-8, "refine": bool(args.refine),
                       "l2": "256 MiB flush write before every timed solve (excluded from step time)",
                       "parallelism": "replicas" if ws > 1 else "single"},
@@ -444,6 +450,8 @@ def adjoint_leg(dev):
     info = {}
     E, g2, g3 = A.ccsd_energy_and_gradient(L_BENCH, holes, C2, C3, device=dev, precision="mixed", eps=1e-10,
                                            mixed_eps=1e-8, lambda_tol=1e-8, info=info)
+    from nulattice_b200 import tune as T
+    T.tune(info["engine"])
     # timed on the warm engine (buffers allocated, step graphs captured):
     # forward and Lambda solves measured the same way, median of three
     runs = []

@@ -61,7 +61,11 @@ typedef struct {
     int32_t uniform_nh;           /* every channel has nh1 == nh2 == this (0: not uniform) */
     int32_t diag_ladders;         /* 1: both ladders only couple a pair to itself */
     int32_t max_fpp_offdiag;      /* most off-diagonal entries in one f_pp row */
-    int32_t reserved;             /* 0 */
+    int32_t tune;                 /* launch shapes, 0 = defaults (threads x resident blocks/SM):
+                                     bits 0-3 lattice T2 kernel, FP32 (0 256x2, 1 512x1, 2 384x1);
+                                     bits 4-7 lattice Lambda row pass, FP32 (0 256x2, 1 512x1);
+                                     bits 8-15 Lambda column-pass row chunks (0: automatic);
+                                     bits 16-19 lattice T2 kernel, FP64 (0 512x1, 1 256x1) */
     const nlb_channel *chan;      /* [n_channels] */
     const int64_t *t2_end;        /* [n_channels] cumulative end of each block */
     const int64_t *g_end;         /* [n_channels] cumulative end of Ga blocks */

@@ -35,7 +35,7 @@ class StructProblem(ctypes.Structure):
     _fields_ = [("p", c_int32), ("h", c_int32), ("n_labels", c_int32), ("n_channels", c_int32)] + \
                [(n, c_int64) for n in ("n_t2", "n_g", "n_f2", "n_rows", "n_t1c", "n_xc")] + \
                [("max_row", c_int32), ("max_nh", c_int32), ("uniform_nh", c_int32), ("diag_ladders", c_int32),
-                ("max_fpp_offdiag", c_int32), ("reserved", c_int32)] + [
+                ("max_fpp_offdiag", c_int32), ("tune", c_int32)] + [
         (n, c_void_p) for n in ("chan", "t2_end", "g_end", "row_end", "t1c_base", "xc_base",
                                 "p_ord", "h_ord", "p_label", "h_label",
                                 "p_loc", "h_loc", "p_base", "h_base", "fpp_ptr", "fpp_col", "fpp_val",

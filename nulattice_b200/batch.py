@@ -165,10 +165,21 @@ class BatchScan:
     iteration counts."""
 
     def __init__(self, instances, device="cuda:0", mixing=0.5, mixed_eps=1e-8, eps=1e-10, lambda_tol_fp32=1e-6,
-                 lambda_tol=1e-8, max_steps=500, lambda_max_steps=500, max_diis=8, chunk=8):
+                 lambda_tol=1e-8, max_steps=500, lambda_max_steps=500, max_diis=8, chunk=8, autotune=True):
         self.dev = torch.device(device)
         self.instances = [_Instance(A, L, C2, C3, self.dev, max_diis) for (A, L, C2, C3) in instances]
         L_ = _lib.lib()
+        # launch shapes: tuned once per (L, A) class on its first instance
+        self.tuning = {}
+        if autotune:
+            from . import tune as _tune
+            for x in self.instances:
+                cls = (x.L, x.A)
+                if cls not in self.tuning:
+                    info = {}
+                    _tune.tune(x.eng, info=info)
+                    self.tuning[cls] = (int(x.eng.prob.tune), info)
+                x.eng.prob.tune = self.tuning[cls][0]
         items = (_lib.BatchItem * len(self.instances))(*[x.item() for x in self.instances])
         self._items = items
         cfg = _lib.BatchConfig(mixing=mixing, mixed_eps=mixed_eps, eps=eps, lambda_tol_fp32=lambda_tol_fp32,

@@ -942,11 +942,16 @@ int64_t smem_limit();
 int blocks_per_sm(const void* fn, int64_t smem, int threads = kThreads) {
     for (int k = 0; k < g_nocc; ++k)
         if (g_occ[k].fn == fn && g_occ[k].smem == smem) return g_occ[k].bps;
-    // raise the limit to the device maximum for every kernel that takes
-    // dynamic shared memory: the 48 KB default counts static shared memory
-    // too, and lowering the limit for a smaller problem would break launches
-    // (and captured graphs) of a larger one
-    if (smem > 0) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem_limit() - 1024));
+    // raise the limit to the device maximum (less the kernel's static shared
+    // memory) for every kernel that takes dynamic shared memory: the 48 KB
+    // default counts static shared memory too, and lowering the limit for a
+    // smaller problem would break launches (and captured graphs) of a larger one
+    if (smem > 0) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess)
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(smem_limit() - (int64_t)fa.sharedSizeBytes));
+    }
     int bps = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, (size_t)smem) != cudaSuccess || bps <= 0)
         bps = 1;
@@ -982,9 +987,6 @@ int64_t smem_limit() {
     return g_smem_limit;
 }
 
-constexpr int kLatThreadsF32 = 256;   // 5 groups of 49 hole pairs, 2 blocks per SM
-constexpr int kLatThreadsF64 = 512;   // 10 groups, 1 block per SM
-
 // The lattice path of the T2 update applies (7 holes per label, diagonal
 // ladders, short f_pp rows) and its shared memory fits.
 bool use_lat(const nlb_struct_problem* P, size_t el) {
@@ -1003,6 +1005,18 @@ int valid(const nlb_struct_problem* P, const nlb_struct_state* S) {
     return NLB_OK;
 }
 
+// The lattice T2 kernel with NT threads per block (NT / 49 hole-pair groups)
+// and at least MINB resident blocks per SM.
+template <typename T, int NT, int MINB>
+void launch_lat(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t st) {
+    const int64_t sm = lat_smem(P->max_row, 7, sizeof(T)).total;
+    auto kern = k_t2_lat<T, 7, NT, MINB>;
+    const int bps = blocks_per_sm(reinterpret_cast<const void*>(kern), sm, NT);
+    int64_t grid = (int64_t)num_sms() * bps;
+    if (grid > P->n_rows) grid = P->n_rows;
+    kern<<<(unsigned)grid, NT, (size_t)sm, st>>>(*P, *S);
+}
+
 template <typename T>
 void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, cudaStream_t st) {
     switch (stage) {
@@ -1016,14 +1030,17 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
             break;
         case NLB_STAGE_T2:
             if (P->n_t2 > 0 && use_lat(P, sizeof(T))) {
-                constexpr int nt = sizeof(T) == 4 ? kLatThreadsF32 : kLatThreadsF64;
-                constexpr int minb = sizeof(T) == 4 ? 2 : 1;
-                const int64_t sm = lat_smem(P->max_row, 7, sizeof(T)).total;
-                auto kern = k_t2_lat<T, 7, nt, minb>;
-                const int bps = blocks_per_sm(reinterpret_cast<const void*>(kern), sm, nt);
-                int64_t grid = (int64_t)num_sms() * bps;
-                if (grid > P->n_rows) grid = P->n_rows;
-                kern<<<(unsigned)grid, nt, (size_t)sm, st>>>(*P, *S);
+                // launch shape from the problem's tuning word (FP32: bits 0-3, FP64:
+                // bits 16-19), see nlb_struct_problem
+                if constexpr (sizeof(T) == 4) {
+                    const int v = P->tune & 15;
+                    if (v == 1) launch_lat<T, 512, 1>(P, S, st);
+                    else if (v == 2) launch_lat<T, 384, 1>(P, S, st);
+                    else launch_lat<T, 256, 2>(P, S, st);
+                } else {
+                    if (((P->tune >> 16) & 15) == 1) launch_lat<T, 256, 1>(P, S, st);
+                    else launch_lat<T, 512, 1>(P, S, st);
+                }
             } else if (P->n_t2 > 0) {
                 const int64_t sm = smem_bytes(P, sizeof(T) == 8 ? NLB_F64 : NLB_F32);
                 auto kern = P->uniform_nh == 7 ? k_t2_rows<T, 7> : P->uniform_nh == 1 ? k_t2_rows<T, 1>

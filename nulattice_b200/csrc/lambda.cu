@@ -903,11 +903,16 @@ int lat_bps(const void* fn, int64_t smem, int threads) {
     static int vals[16] = {};
     for (int k = 0; k < 16; ++k)
         if (fns[k] == fn && sms[k] == smem) return vals[k];
-    // raise the limit to the device maximum for every kernel that takes
-    // dynamic shared memory: the 48 KB default counts static shared memory
-    // too, and lowering the limit for a smaller problem would break launches
-    // (and captured graphs) of a larger one
-    if (smem > 0) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(optin_smem() - 1024));
+    // raise the limit to the device maximum (less the kernel's static shared
+    // memory) for every kernel that takes dynamic shared memory: the 48 KB
+    // default counts static shared memory too, and lowering the limit for a
+    // smaller problem would break launches (and captured graphs) of a larger one
+    if (smem > 0) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess)
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(optin_smem() - (int64_t)fa.sharedSizeBytes));
+    }
     int bps = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, threads, (size_t)smem) != cudaSuccess || bps < 1)
         bps = 1;
@@ -928,6 +933,16 @@ int col_chunks(const nlb_struct_problem* P) {
     return (int)(n < 1 ? 1 : n);
 }
 
+template <typename T, int NT, int MINB>
+void launch_llat(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_t s) {
+    const int64_t sm = llat_smem(P->max_row, NT / kLHP, sizeof(T)).total;
+    auto kern = k_l_lat<T, NT, MINB>;
+    const int bps = lat_bps(reinterpret_cast<const void*>(kern), sm, NT);
+    int64_t grid = (int64_t)num_sms_l() * bps;
+    if (grid > P->n_rows) grid = P->n_rows;
+    kern<<<(unsigned)grid, NT, (size_t)sm, s>>>(*P, *S);
+}
+
 template <typename T>
 int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_t s) {
     constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
@@ -935,20 +950,22 @@ int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_
     k_l_u<<<grid_l(32 * hh + (int64_t)P->p * P->h), kThreads, 0, s>>>(*P, *S);
     cudaMemsetAsync(S->ha, 0, sizeof(T) * (size_t)P->n_g, s);
     {
-        // every label has the same particle count on the lattice path
+        // every label has the same particle count on the lattice path;
+        // row chunks from the tuning word (bits 8-15, 0: automatic)
         constexpr int NB = kColThreads / kLHP;
-        const int nchunk = col_chunks(P);
+        const int tuned = (P->tune >> 8) & 255;
+        const int64_t np1 = P->max_row / kLHP;
+        const int nchunk = tuned > 0 ? (int)(tuned < np1 ? tuned : np1) : col_chunks(P);
         const int64_t np2 = P->max_row / kLHP;
         const int64_t items = (np2 + NB - 1) / NB * nchunk * P->n_channels;
         k_l_cols<T, kColThreads><<<(unsigned)items, kColThreads, 0, s>>>(*P, *S, nchunk);
     }
-    {
-        const int64_t sm = llat_smem(P->max_row, kLatThreads / kLHP, sizeof(T)).total;
-        auto kern = k_l_lat<T, kLatThreads, MINB>;
-        const int bps = lat_bps(reinterpret_cast<const void*>(kern), sm, kLatThreads);
-        int64_t grid = (int64_t)num_sms_l() * bps;
-        if (grid > P->n_rows) grid = P->n_rows;
-        kern<<<(unsigned)grid, kLatThreads, (size_t)sm, s>>>(*P, *S);
+    // row-pass launch shape from the tuning word (bits 4-7)
+    if constexpr (sizeof(T) == 4) {
+        if (((P->tune >> 4) & 15) == 1) launch_llat<T, 512, 1>(P, S, s);
+        else launch_llat<T, kLatThreads, MINB>(P, S, s);
+    } else {
+        launch_llat<T, kLatThreads, MINB>(P, S, s);
     }
     if (cudaPeekAtLastError() != cudaSuccess) return lcheck("nlb_lambda_step");
     k_l_t1<<<grid_l((int64_t)P->p * P->h), kThreads, 0, s>>>(*P, *S);
