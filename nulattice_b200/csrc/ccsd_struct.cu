@@ -707,40 +707,58 @@ constexpr int kMaxDiis = 10;
 
 template <typename T, int M>
 __global__ void __launch_bounds__(kThreads) k_diis_gram(nlb_struct_problem P, nlb_struct_state S) {
+    // FP32 error vectors: products and per-thread partial sums in FP32 (the
+    // sums cover a few hundred elements, relative error ~1e-5, well inside
+    // what the extrapolation needs), block and grid sums in FP64; FP64
+    // vectors: FP64 throughout.  Two elements per thread and step keep
+    // 2M loads in flight.
+    using A = T;
     nlb_ctrl* c = S.ctrl;
     if (!c->diis_pulse) return;
     constexpr int NP = M * (M + 1) / 2;
-    double acc[NP];
+    A acc[NP];   // sum of w/4 * e_s e_t: T1 entries weigh 1/4 here, T2 entries 1
 #pragma unroll
-    for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+    for (int k = 0; k < NP; ++k) acc[k] = A(0);
     const int64_t n1 = (int64_t)P.p * P.h;
     const int64_t n2 = c->ccs ? 0 : P.n_t2;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t e = tid0; e < n1; e += stride) {
+        A v[M];
+#pragma unroll
+        for (int s = 0; s < M; ++s) v[s] = (A)(0.5 * S.diis_t1[(int64_t)s * n1 + e]);
+        int k = 0;
+#pragma unroll
+        for (int s = 0; s < M; ++s)
+#pragma unroll
+            for (int t = s; t < M; ++t) acc[k++] += v[s] * v[t];
+    }
+    // T2 part, weight 4 (four images per stored amplitude)
     const T* E2 = static_cast<const T*>(S.diis_t2);
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n1 + n2; e += stride) {
-        double v[M];
-        double w;
-        if (e < n1) {
+    for (int64_t e = tid0; e < n2; e += 2 * stride) {
+        const int64_t e2 = e + stride;
+        const bool two = e2 < n2;
+        T v[M], u[M];
 #pragma unroll
-            for (int s = 0; s < M; ++s) v[s] = S.diis_t1[(int64_t)s * n1 + e];
-            w = 1.0;
-        } else {
-#pragma unroll
-            for (int s = 0; s < M; ++s) v[s] = (double)E2[(int64_t)s * P.n_t2 + (e - n1)];
-            w = 4.0;
+        for (int s = 0; s < M; ++s) {
+            v[s] = E2[(int64_t)s * P.n_t2 + e];
+            u[s] = two ? E2[(int64_t)s * P.n_t2 + e2] : T(0);
         }
         int k = 0;
 #pragma unroll
         for (int s = 0; s < M; ++s)
 #pragma unroll
-            for (int t = s; t < M; ++t) acc[k++] += w * v[s] * v[t];
+            for (int t = s; t < M; ++t) {
+                acc[k] += v[s] * v[t] + u[s] * u[t];
+                ++k;
+            }
     }
     // warp reductions, then one shared-memory pass per warp
     __shared__ double red[kThreads / 32][NP];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-        const double v = warp_sum(acc[k]);
+        const double v = warp_sum(4.0 * (double)acc[k]);
         if (lane == 0) red[wid][k] = v;
     }
     __syncthreads();

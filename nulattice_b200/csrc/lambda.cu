@@ -475,10 +475,13 @@ __global__ void k_l_setup_lat(nlb_struct_problem P, nlb_lambda_state S) {
 //   T[k', i'] (g1)  += Lam[a'][b'][i', j'] B[a'][b'][k', j']
 //   T[k', j'] (g2)  += Lam[a'][b'][i', j'] B[a'][b'][i', k']
 // and adds its partial sums with atomics (Ha is zeroed before the pass).
+constexpr int kColRows = 256;          // most rows in one chunk of the column pass
+
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lambda_state S, int nchunk) {
     constexpr int NB = NT / kLHP;
     __shared__ double sv[NT][kLH + 1];    // per-thread partial sums, one kind at a time
+    __shared__ __align__(16) unsigned char smem_raw[kColRows * (8 + NB) * sizeof(T)];
     const nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
     const T* __restrict__ Lm = static_cast<const T*>(S.lam2[c->parity]);
@@ -510,32 +513,44 @@ __global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lamb
 #pragma unroll
     for (int k = 0; k < kLH; ++k) { hak[k] = T(0); ys[k] = T(0); tt1[k] = T(0); tt2[k] = T(0); }
     const int64_t col = (int64_t)bp * kLHP + hp;   // element offset of (b', hp) in a row
+    // the chunk's t1[a', H_g1] rows (8-padded) and pp ladder entries (a', b'),
+    // staged once per block
+    T* st1 = reinterpret_cast<T*>(smem_raw);                 // [nr][8]
+    T* scpp = st1 + kColRows * 8;                            // [nr][NB]
+    const int nr = a1 - a0;
+    {
+        const double* t1a = PV.t1c + P.t1c_base[ch.g1];
+        const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off;
+        const double* pval = P.pp_val + ch.pp_col_off;
+        for (int w = tid; w < nr * 8; w += NT) {
+            const int r = w >> 3, k = w & 7;
+            st1[w] = k < kLH ? (T)t1a[(a0 + r) * kLH + k] : T(0);
+        }
+        for (int w = tid; w < nr * NB; w += NT) {
+            const int r = w / NB, g = w - r * NB;
+            const int b2 = bb * NB + g;
+            T v = T(0);
+            if (b2 < ch.np2) {
+                const int ab = (a0 + r) * ch.np2 + b2;
+                if (pptr[ab + 1] > pptr[ab]) v = (T)pval[pptr[ab]];
+            }
+            scpp[w] = v;
+        }
+    }
+    __syncthreads();
     if (act) {
         const int32_t* hptr = P.hh_ptr + ch.hh_ptr_off;
-        const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off + bp;
-        const double* pval = P.pp_val + ch.pp_col_off;
         const T shh = (hptr[hp + 1] > hptr[hp]) ? (T)P.hh_val[ch.hh_col_off + hptr[hp]] : T(0);
-        const double* t1a = PV.t1c + P.t1c_base[ch.g1];
         const T* gbr = gb + (ci ? P.row_end[ci - 1] : 0) * (int64_t)(kLH * kLHP) + hp;
         const T* Lc = Lm + ch.offset + col;
         const T* Bb = B + ch.offset + (int64_t)bp * kLHP;   // block (a', b') of t2 at + a' rowlen
         // no barrier in the loop: every operand is an independent load (the
-        // t2 block values come from L1 after the first touch)
-        for (int ap = a0; ap < a1; ++ap) {
-            const int64_t ro = (int64_t)ap * rowlen;
-            const T x = Lc[ro];
-            const T* blk = Bb + ro;
-            T bc[kLH], br[kLH], g[kLH], ta[kLH];
-#pragma unroll
-            for (int k = 0; k < kLH; ++k) {
-                bc[k] = __ldg(blk + k * kLH + jp);
-                br[k] = __ldg(blk + ip * kLH + k);
-                g[k] = __ldg(gbr + (int64_t)ap * (kLH * kLHP) + k * kLHP);
-                ta[k] = (T)__ldg(t1a + ap * kLH + k);
-            }
-            const int ab = ap * ch.np2;
-            const int q0 = __ldg(pptr + ab), q1 = __ldg(pptr + ab + 1);
-            const T cpp = (q1 > q0) ? (T)__ldg(pval + q0) : T(0);
+        // t2 block values come from L1 after the first touch); two rows per
+        // step keep twice the loads in flight
+        auto row = [&](int r, T x, const T (&bc)[kLH], const T (&br)[kLH], const T (&g)[kLH]) {
+            T ta[8];
+            lds8(st1 + r * 8, ta);
+            const T cpp = scpp[r * NB + grp];
 #pragma unroll
             for (int k = 0; k < kLH; ++k) {
                 hak[k] += ta[k] * x;
@@ -543,7 +558,39 @@ __global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lamb
                 tt1[k] += x * bc[k];
                 tt2[k] += x * br[k];
             }
-            ylt += x * (shh + cpp) * ta[ip];
+            T tai = ta[0];
+#pragma unroll
+            for (int k = 1; k < kLH; ++k) tai = (ip == k) ? ta[k] : tai;
+            ylt += x * (shh + cpp) * tai;
+        };
+        int r = 0;
+        for (; r + 1 < nr; r += 2) {
+            const int64_t ro0 = (int64_t)(a0 + r) * rowlen, ro1 = ro0 + rowlen;
+            const T x0 = Lc[ro0], x1 = Lc[ro1];
+            T bc0[kLH], br0[kLH], g0[kLH], bc1[kLH], br1[kLH], g1[kLH];
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) {
+                bc0[k] = __ldg(Bb + ro0 + k * kLH + jp);
+                br0[k] = __ldg(Bb + ro0 + ip * kLH + k);
+                g0[k] = __ldg(gbr + (int64_t)(a0 + r) * (kLH * kLHP) + k * kLHP);
+                bc1[k] = __ldg(Bb + ro1 + k * kLH + jp);
+                br1[k] = __ldg(Bb + ro1 + ip * kLH + k);
+                g1[k] = __ldg(gbr + (int64_t)(a0 + r + 1) * (kLH * kLHP) + k * kLHP);
+            }
+            row(r, x0, bc0, br0, g0);
+            row(r + 1, x1, bc1, br1, g1);
+        }
+        if (r < nr) {
+            const int64_t ro0 = (int64_t)(a0 + r) * rowlen;
+            const T x0 = Lc[ro0];
+            T bc0[kLH], br0[kLH], g0[kLH];
+#pragma unroll
+            for (int k = 0; k < kLH; ++k) {
+                bc0[k] = __ldg(Bb + ro0 + k * kLH + jp);
+                br0[k] = __ldg(Bb + ro0 + ip * kLH + k);
+                g0[k] = __ldg(gbr + (int64_t)(a0 + r) * (kLH * kLHP) + k * kLHP);
+            }
+            row(r, x0, bc0, br0, g0);
         }
 #pragma unroll
         for (int k = 0; k < kLH; ++k) atomicAdd(&ha[ch.ga_off + (int64_t)k * rowlen + col], hak[k]);
@@ -955,7 +1002,9 @@ int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_
         constexpr int NB = kColThreads / kLHP;
         const int tuned = (P->tune >> 8) & 255;
         const int64_t np1 = P->max_row / kLHP;
-        const int nchunk = tuned > 0 ? (int)(tuned < np1 ? tuned : np1) : col_chunks(P);
+        int nchunk = tuned > 0 ? (int)(tuned < np1 ? tuned : np1) : col_chunks(P);
+        const int need = (int)((np1 + kColRows - 1) / kColRows);   // rows of a chunk fit the staging
+        if (nchunk < need) nchunk = need;
         const int64_t np2 = P->max_row / kLHP;
         const int64_t items = (np2 + NB - 1) / NB * nchunk * P->n_channels;
         k_l_cols<T, kColThreads><<<(unsigned)items, kColThreads, 0, s>>>(*P, *S, nchunk);
