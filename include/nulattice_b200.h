@@ -250,7 +250,8 @@ int nlb_lambda_coupling(const nlb_struct_problem *prob, const nlb_lambda_state *
 /* ---------------------------------------------------------------------
  * Batched scan (no counterpart in the reference): many structured problems
  * of uneven size solved, with their coupling derivatives, in ONE CUDA graph
- * launch.  The graph holds four device-side loops (conditional WHILE nodes):
+ * launch (one instance and the forward phases alone give a whole solve as
+ * one launch, no host round trips).  The graph holds four device-side loops (conditional WHILE nodes):
  * forward FP32 to mixed_eps, forward FP64 to eps, Lambda FP32 to
  * lambda_tol_fp32 (lattice instances) and Lambda FP64 to lambda_tol; each
  * loop body is one branch per instance (chunk steps, DIIS pulses included).
@@ -269,10 +270,15 @@ typedef struct {
                                          FP32 forward iterations */
 } nlb_batch_item;
 
+enum { NLB_PHASE_FWD32 = 1, NLB_PHASE_FWD64 = 2, NLB_PHASE_LAMBDA = 4 };
+
 typedef struct {
     double mixing, mixed_eps, eps, lambda_tol_fp32, lambda_tol;
     int32_t max_steps, max_diis, lambda_max_steps;
     int32_t chunk;                    /* steps per loop iteration; a multiple of max_diis */
+    int32_t phases;                   /* NLB_PHASE_* bits: forward FP32 (to mixed_eps), forward FP64 (to eps,
+                                         from the FP32 result when both), Lambda (needs FP64 forward) */
+    int32_t criterion;                /* NLB_CRIT_SOA / NLB_CRIT_NUMPY for the forward phases */
 } nlb_batch_config;
 
 /* Capture and instantiate the batch graph (buffers stay caller-owned). */

@@ -73,7 +73,10 @@ class BatchItem(ctypes.Structure):
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [(n, c_double) for n in ("mixing", "mixed_eps", "eps", "lambda_tol_fp32", "lambda_tol")] + [
-        (n, c_int32) for n in ("max_steps", "max_diis", "lambda_max_steps", "chunk")]
+        (n, c_int32) for n in ("max_steps", "max_diis", "lambda_max_steps", "chunk", "phases", "criterion")]
+
+
+NLB_PHASE_FWD32, NLB_PHASE_FWD64, NLB_PHASE_LAMBDA = 1, 2, 4
 
 
 class ContractDesc(ctypes.Structure):

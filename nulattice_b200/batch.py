@@ -184,7 +184,9 @@ class BatchScan:
         self._items = items
         cfg = _lib.BatchConfig(mixing=mixing, mixed_eps=mixed_eps, eps=eps, lambda_tol_fp32=lambda_tol_fp32,
                                lambda_tol=lambda_tol, max_steps=max_steps, max_diis=max_diis,
-                               lambda_max_steps=lambda_max_steps, chunk=chunk)
+                               lambda_max_steps=lambda_max_steps, chunk=chunk,
+                               phases=_lib.NLB_PHASE_FWD32 | _lib.NLB_PHASE_FWD64 | _lib.NLB_PHASE_LAMBDA,
+                               criterion=_lib.NLB_CRIT_SOA)
         self.cfg = cfg
         handle = ctypes.c_void_p()
         torch.cuda.synchronize(self.dev)

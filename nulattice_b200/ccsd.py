@@ -230,6 +230,48 @@ class StructuredEngine:
         raw = b["ctrl"].cpu().numpy().tobytes()
         return _lib.Ctrl.from_buffer_copy(raw)
 
+    # -- a whole solve as one graph launch --------------------------------
+    def device_loop(self, t1_init, e0, phases, eps, mixed_eps, mixing, max_steps, criterion, max_diis, chunk):
+        """Launch the whole forward solve (FP32 and/or FP64 phases) as one CUDA
+        graph with device-side loops (the batch machinery with one instance);
+        returns (ctrl of the last phase, its buffers, out[8])."""
+        import ctypes
+        L = _lib.lib()
+        key = ("loop", phases, float(eps), float(mixed_eps), float(mixing), int(max_steps), int(criterion),
+               int(max_diis), int(chunk), float(e0))
+        if not hasattr(self, "_loops"):
+            self._loops = {}
+            self._loop_t1 = torch.zeros(self.plan.p * self.plan.h, dtype=torch.float64, device=self.dev)
+            self._loop_out = torch.zeros(8, dtype=torch.float64, device=self.dev)
+        b32 = self.buffers(_lib.NLB_F32, max_diis) if phases & _lib.NLB_PHASE_FWD32 else None
+        b64 = self.buffers(_lib.NLB_F64, max_diis) if phases & _lib.NLB_PHASE_FWD64 else None
+        if key not in self._loops:
+            it = _lib.BatchItem()
+            it.prob = ctypes.pointer(self.prob)
+            if b32 is not None:
+                it.f32 = b32["state"]
+            if b64 is not None:
+                it.f64 = b64["state"]
+            it.t1_init = self._loop_t1.data_ptr()
+            it.e0 = float(e0)
+            it.out = self._loop_out.data_ptr()
+            items = (_lib.BatchItem * 1)(it)
+            cfg = _lib.BatchConfig(mixing=mixing, mixed_eps=mixed_eps, eps=eps, lambda_tol_fp32=0.0, lambda_tol=0.0,
+                                   max_steps=max_steps, max_diis=max_diis, lambda_max_steps=0, chunk=chunk,
+                                   phases=phases, criterion=criterion)
+            handle = ctypes.c_void_p()
+            _lib.check(L.nlb_batch_create(items, 1, ctypes.byref(cfg), ctypes.byref(handle)), "loop create")
+            self._loops[key] = (handle, items)
+        handle = self._loops[key][0]
+        self._loop_t1.copy_(t1_init.reshape(-1))
+        stream = torch.cuda.current_stream(self.dev)
+        _lib.check(L.nlb_batch_launch(handle, ctypes_void(stream.cuda_stream)), "loop launch")
+        b = b64 if b64 is not None else b32
+        c = self.read_ctrl(b)
+        self.last_fp32_ctrl = self.read_ctrl(b32) if (b32 is not None and b64 is not None) else \
+            (c if b32 is not None else None)
+        return c, b, self._loop_out.cpu().numpy()
+
     # -- one phase of iterations ------------------------------------------
     def run(self, b, t1_init, t2c_init, e0, eps, mixing, max_steps, criterion, max_diis, ccs,
             verbose=False, sync_every=16, step_offset=0, t2_events=None, graph=True):
@@ -416,7 +458,27 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
     sp = ctypes_void(torch.cuda.current_stream(dev).cuda_stream)
     iters = 0
     t0 = time.perf_counter()
-    if precision == "mixed":
+    if t2_events is None and not verbose and not ccs:
+        # the whole solve as one graph launch: device-side loops, no host
+        # round trip per chunk of steps
+        chunk = diis if diis else sync_every
+        while diis and chunk < 8:
+            chunk += diis
+        me = float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)
+        if precision == "mixed":
+            phases = _lib.NLB_PHASE_FWD32 | (_lib.NLB_PHASE_FWD64 if refine else 0)
+        else:
+            phases = _lib.NLB_PHASE_FWD64
+        c, b, out = eng.device_loop(t1_dev, e0, phases, eps, me, mixing, maxSteps, crit, diis, chunk)
+        iters = int(out[4])
+        # kernels run: five per step, four per DIIS pulse, the prologue and report
+        eng.launches += 5 * iters + (4 * (iters // diis) if diis else 0) + 3
+        if precision == "mixed":
+            info["mixed_iters"] = int(out[7])
+            info["mixed_energy"] = eng.last_fp32_ctrl.e_last
+            if refine and phases & _lib.NLB_PHASE_FWD64:
+                info["refine_iters"] = iters - int(out[7])
+    elif precision == "mixed":
         b32 = eng.buffers(_lib.NLB_F32, diis)
         me = float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)
         c = eng.run(b32, t1_dev, None, e0, me, mixing, maxSteps, crit, diis, ccs, verbose, sync_every,

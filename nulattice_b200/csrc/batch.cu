@@ -66,7 +66,7 @@ __global__ void k_batch_cond(cudaGraphConditionalHandle h, const cudaGraphCondit
 // energy; an FP32 phase that did not converge passes its status on.
 __global__ void k_batch_fwd_handoff(const nlb_ctrl* c32, nlb_ctrl* c64, const nlb_struct_state s32,
                                     nlb_struct_state s64, int64_t n1, int64_t n2, double eps, double mixing,
-                                    int max_steps, int max_diis) {
+                                    int max_steps, int max_diis, int criterion) {
     const int par = c32->parity;
     const double* t1 = s32.t1[par];
     const float* t2 = static_cast<const float*>(s32.t2[par]);
@@ -84,7 +84,7 @@ __global__ void k_batch_fwd_handoff(const nlb_ctrl* c32, nlb_ctrl* c64, const nl
         for (int k = 0; k < 121; ++k) c64->gram[k] = 0.0;
         const int left = max_steps - c32->iter;
         c64->parity = 0; c64->iter = 0; c64->max_steps = left;
-        c64->criterion = NLB_CRIT_SOA; c64->max_diis = max_diis; c64->diis_count = 0; c64->diis_pulse = 0;
+        c64->criterion = criterion; c64->max_diis = max_diis; c64->diis_count = 0; c64->diis_pulse = 0;
         c64->diis_applied = 0; c64->ccs = 0;
         c64->status = (c32->status == NLB_CONVERGED) ? (left > 0 ? NLB_RUNNING : NLB_MAX_ITER) : c32->status;
     }
@@ -130,18 +130,20 @@ __global__ void k_batch_gate(const nlb_ctrl* fwd, nlb_ctrl* lam) {
     if (threadIdx.x == 0 && blockIdx.x == 0 && fwd->status != NLB_CONVERGED) lam->status = fwd->status;
 }
 
-// out[0] E_corr, [3] forward status, [4] forward iterations (both phases),
-// [5] Lambda status, [6] Lambda iterations (both phases), [7] FP32 forward
-// iterations; [1], [2] hold the coupling terms (nlb_lambda_coupling).
+// out[0] E_corr of the last forward phase, [3] its status, [4] forward
+// iterations (both phases), [5] Lambda status, [6] Lambda iterations (both
+// phases), [7] FP32 forward iterations; [1], [2] hold the coupling terms
+// (nlb_lambda_coupling).  Phases that did not run are passed as null.
 __global__ void k_batch_report(const nlb_ctrl* c32, const nlb_ctrl* c64, const nlb_ctrl* l32, const nlb_ctrl* l64,
                                double* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    out[0] = c64->e_last;
-    out[3] = (double)c64->status;
-    out[4] = (double)(c32->iter + c64->iter);
-    out[5] = (double)l64->status;
-    out[6] = (double)((l32 ? l32->iter : 0) + l64->iter);
-    out[7] = (double)c32->iter;
+    const nlb_ctrl* last = c64 ? c64 : c32;
+    out[0] = last->e_last;
+    out[3] = (double)last->status;
+    out[4] = (double)((c32 ? c32->iter : 0) + (c64 ? c64->iter : 0));
+    out[5] = l64 ? (double)l64->status : 0.0;
+    out[6] = (double)((l32 ? l32->iter : 0) + (l64 ? l64->iter : 0));
+    out[7] = c32 ? (double)c32->iter : 0.0;
 }
 
 struct Batch {
@@ -326,43 +328,64 @@ int build(Batch* b, const nlb_batch_item* items, const nlb_batch_config& cfg) {
     }
     const int cap_f = (cfg.max_steps + chunk - 1) / chunk + 1;
     const int cap_l = (cfg.lambda_max_steps + chunk - 1) / chunk + 1;
+    const bool f32 = cfg.phases & NLB_PHASE_FWD32, f64 = cfg.phases & NLB_PHASE_FWD64,
+               lam = cfg.phases & NLB_PHASE_LAMBDA;
     cudaGraphNode_t prev = nullptr;
     int rc;
-    // prologue: start amplitudes and control blocks of the FP32 forward phase
+    // prologue: start amplitudes and control block of the first forward phase
     rc = append_segment(b, &prev, [&]() {
         int r = bcuda(cudaMemsetAsync(counters, 0, 4 * sizeof(int), b->cs), "batch counters");
         if (r) return r;
         return parallel(b, [&](int i, cudaStream_t s) {
             const nlb_batch_item& it = items[i];
+            const nlb_struct_state& st = f32 ? it.f32 : it.f64;
             const int64_t n1 = (int64_t)it.prob->p * it.prob->h, n2 = it.prob->n_t2;
-            int q = bcuda(cudaMemcpyAsync(it.f32.t1[0], it.t1_init, sizeof(double) * n1, cudaMemcpyDeviceToDevice, s),
+            int q = bcuda(cudaMemcpyAsync(st.t1[0], it.t1_init, sizeof(double) * n1, cudaMemcpyDeviceToDevice, s),
                           "batch t1 start");
-            if (!q && n2 > 0) q = bcuda(cudaMemsetAsync(it.f32.t2[0], 0, sizeof(float) * n2, s), "batch t2 start");
-            if (!q) q = nlb_struct_ctrl_init(it.f32.ctrl, cfg.mixed_eps, cfg.mixing, cfg.max_steps, NLB_CRIT_SOA, md, 0,
-                                             it.e0, s);
+            if (!q && n2 > 0)
+                q = bcuda(cudaMemsetAsync(st.t2[0], 0, (f32 ? sizeof(float) : sizeof(double)) * n2, s), "batch t2 start");
+            if (!q) q = nlb_struct_ctrl_init(st.ctrl, f32 ? cfg.mixed_eps : cfg.eps, cfg.mixing, cfg.max_steps,
+                                             cfg.criterion, md, 0, it.e0, s);
             return q;
         });
     });
     if (rc) return rc;
-    // forward, FP32
-    rc = append_loop(b, &prev, lists, handles, counters + 0, cap_f,
-                     [&](int i, cudaStream_t s) { return steps(items[i], &items[i].f32, chunk, md, s); });
-    if (rc) return rc;
-    // handoff to FP64
-    rc = append_segment(b, &prev, [&]() {
-        return parallel(b, [&](int i, cudaStream_t s) {
-            const nlb_batch_item& it = items[i];
-            const int64_t n1 = (int64_t)it.prob->p * it.prob->h, n2 = it.prob->n_t2;
-            k_batch_fwd_handoff<<<grid_for(n1 + n2), kT, 0, s>>>(it.f32.ctrl, it.f64.ctrl, it.f32, it.f64, n1, n2,
-                                                               cfg.eps, cfg.mixing, cfg.max_steps, md);
-            return bcuda(cudaGetLastError(), "batch forward handoff");
+    if (f32) {
+        // forward, FP32
+        rc = append_loop(b, &prev, lists, handles, counters + 0, cap_f,
+                         [&](int i, cudaStream_t s) { return steps(items[i], &items[i].f32, chunk, md, s); });
+        if (rc) return rc;
+    }
+    if (f32 && f64) {
+        // handoff to FP64
+        rc = append_segment(b, &prev, [&]() {
+            return parallel(b, [&](int i, cudaStream_t s) {
+                const nlb_batch_item& it = items[i];
+                const int64_t n1 = (int64_t)it.prob->p * it.prob->h, n2 = it.prob->n_t2;
+                k_batch_fwd_handoff<<<grid_for(n1 + n2), kT, 0, s>>>(it.f32.ctrl, it.f64.ctrl, it.f32, it.f64, n1, n2,
+                                                                   cfg.eps, cfg.mixing, cfg.max_steps, md,
+                                                                   cfg.criterion);
+                return bcuda(cudaGetLastError(), "batch forward handoff");
+            });
         });
-    });
-    if (rc) return rc;
-    // forward, FP64 finish
-    rc = append_loop(b, &prev, lists + n, handles + n, counters + 1, cap_f,
-                     [&](int i, cudaStream_t s) { return steps(items[i], &items[i].f64, chunk, md, s); });
-    if (rc) return rc;
+        if (rc) return rc;
+    }
+    if (f64) {
+        // forward, FP64 (finish)
+        rc = append_loop(b, &prev, lists + n, handles + n, counters + 1, cap_f,
+                         [&](int i, cudaStream_t s) { return steps(items[i], &items[i].f64, chunk, md, s); });
+        if (rc) return rc;
+    }
+    if (!lam) {
+        return append_segment(b, &prev, [&]() {
+            return parallel(b, [&](int i, cudaStream_t s) {
+                const nlb_batch_item& it = items[i];
+                k_batch_report<<<1, 32, 0, s>>>(f32 ? it.f32.ctrl : nullptr, f64 ? it.f64.ctrl : nullptr, nullptr,
+                                               nullptr, it.out);
+                return bcuda(cudaGetLastError(), "batch report");
+            });
+        });
+    }
     // handoff to the Lambda equations
     rc = append_segment(b, &prev, [&]() {
         return parallel(b, [&](int i, cudaStream_t s) {
@@ -421,8 +444,8 @@ int build(Batch* b, const nlb_batch_item* items, const nlb_batch_config& cfg) {
             int q = (int)NLB_OK;
             for (int d = 0; d < 2 && !q; ++d) q = nlb_lambda_coupling(it.prob, &it.l64, it.dw[d], it.dv[d], it.out + 1 + d, s);
             if (!q) {
-                k_batch_report<<<1, 32, 0, s>>>(it.f32.ctrl, it.f64.ctrl, it.l32.dtype ? it.l32.ctrl : nullptr,
-                                               it.l64.ctrl, it.out);
+                k_batch_report<<<1, 32, 0, s>>>(f32 ? it.f32.ctrl : nullptr, it.f64.ctrl,
+                                               it.l32.dtype ? it.l32.ctrl : nullptr, it.l64.ctrl, it.out);
                 q = bcuda(cudaGetLastError(), "batch report");
             }
             return q;
@@ -440,15 +463,26 @@ int nlb_batch_create(const nlb_batch_item* items, int32_t n, const nlb_batch_con
     *handle = nullptr;
     if (cfg->chunk < 1 || (cfg->max_diis > 0 && cfg->chunk % cfg->max_diis != 0))
         return bfail(NLB_ERR_ARG, "nlb_batch_create: chunk must be a positive multiple of max_diis");
+    const int ph = cfg->phases;
+    if (!(ph & (NLB_PHASE_FWD32 | NLB_PHASE_FWD64)) || (ph & ~7) ||
+        ((ph & NLB_PHASE_LAMBDA) && !(ph & NLB_PHASE_FWD64)))
+        return bfail(NLB_ERR_ARG, "nlb_batch_create: phases need a forward phase; Lambda needs the FP64 forward phase");
+    if (cfg->criterion != NLB_CRIT_SOA && cfg->criterion != NLB_CRIT_NUMPY)
+        return bfail(NLB_ERR_ARG, "nlb_batch_create: bad criterion");
     for (int i = 0; i < n; ++i) {
         const nlb_batch_item& it = items[i];
-        if (!it.prob || !it.t1_init || !it.out || !it.dw[0] || !it.dw[1] || !it.dv[0] || !it.dv[1])
-            return bfail(NLB_ERR_ARG, "nlb_batch_create: null item field");
-        if (it.f32.dtype != NLB_F32 || it.f64.dtype != NLB_F64 || it.l64.dtype != NLB_F64 ||
-            (it.l32.dtype != 0 && it.l32.dtype != NLB_F32))
-            return bfail(NLB_ERR_ARG, "nlb_batch_create: state dtypes must be F32, F64, (F32 or 0), F64");
-        if (it.l64.t1 != it.f64.t1[0] || it.l64.t2 != it.f64.t2[0] || (it.l32.dtype && it.l32.t1 != it.f64.t1[0]))
-            return bfail(NLB_ERR_ARG, "nlb_batch_create: Lambda states must read t1/t2 from buffer 0 of the FP64 state");
+        if (!it.prob || !it.t1_init || !it.out) return bfail(NLB_ERR_ARG, "nlb_batch_create: null item field");
+        if (((ph & NLB_PHASE_FWD32) && it.f32.dtype != NLB_F32) || ((ph & NLB_PHASE_FWD64) && it.f64.dtype != NLB_F64))
+            return bfail(NLB_ERR_ARG, "nlb_batch_create: forward state dtypes must be F32 and F64");
+        if (ph & NLB_PHASE_LAMBDA) {
+            if (!it.dw[0] || !it.dw[1] || !it.dv[0] || !it.dv[1])
+                return bfail(NLB_ERR_ARG, "nlb_batch_create: null derivative ladders");
+            if (it.l64.dtype != NLB_F64 || (it.l32.dtype != 0 && it.l32.dtype != NLB_F32))
+                return bfail(NLB_ERR_ARG, "nlb_batch_create: Lambda state dtypes must be (F32 or 0) and F64");
+            if (it.l64.t1 != it.f64.t1[0] || it.l64.t2 != it.f64.t2[0] || (it.l32.dtype && it.l32.t1 != it.f64.t1[0]))
+                return bfail(NLB_ERR_ARG,
+                             "nlb_batch_create: Lambda states must read t1/t2 from buffer 0 of the FP64 state");
+        }
     }
     Batch* b = new Batch();
     b->n = n;

@@ -128,7 +128,7 @@ def test_lambda_and_batch_struct_layouts():
     from nulattice_b200 import _lib
     assert ctypes.sizeof(_lib.LambdaState) == 120
     assert ctypes.sizeof(_lib.BatchItem) == 480
-    assert ctypes.sizeof(_lib.BatchConfig) == 56
+    assert ctypes.sizeof(_lib.BatchConfig) == 64
 
 
 def test_batch_instances_are_seeded_and_in_range():
