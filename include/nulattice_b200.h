@@ -33,6 +33,10 @@ enum { NLB_OK = 0, NLB_ERR_ARG = 1, NLB_ERR_LAUNCH = 2, NLB_ERR_SIZE = 3, NLB_ER
 enum { NLB_F64 = 0, NLB_F32 = 1 };
 enum { NLB_RUNNING = 0, NLB_CONVERGED = 1, NLB_MAX_ITER = 2, NLB_DIVERGED = 3 };
 enum { NLB_CRIT_SOA = 0, NLB_CRIT_NUMPY = 1 };
+/* Stages of one step (nlb_struct_stage): PREP forms the dressed-Fock tables
+ * and the Ga intermediates in one launch, GTERMS is kept for compatibility
+ * and launches nothing, T2 and T1 update the amplitudes, FINISH tests
+ * convergence. */
 enum { NLB_STAGE_PREP = 0, NLB_STAGE_GTERMS = 1, NLB_STAGE_T2 = 2, NLB_STAGE_T1 = 3, NLB_STAGE_FINISH = 4 };
 
 /* One channel (label pair g1 < g2) of the compact T2: a dense block
@@ -267,7 +271,8 @@ typedef struct {
     const double *dw[2], *dv[2];      /* diagonal derivative ladders of two couplings (FP64) */
     double *out;                      /* [8]: E_corr, coupling term 0, coupling term 1, forward status,
                                          forward iterations, Lambda status, Lambda iterations,
-                                         FP32 forward iterations */
+                                         FP32 forward iterations; without a Lambda phase [1] is the
+                                         parity of the last forward phase and [2] the FP32 energy */
 } nlb_batch_item;
 
 enum { NLB_PHASE_FWD32 = 1, NLB_PHASE_FWD64 = 2, NLB_PHASE_LAMBDA = 4 };

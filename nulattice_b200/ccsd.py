@@ -170,6 +170,7 @@ class StructuredEngine:
             setattr(prob, k, v.data_ptr())
         self.prob = prob
         self._bufs = {}
+        self.cache = {}
         self.launches = 0
 
     # -- buffers ---------------------------------------------------------
@@ -267,10 +268,7 @@ class StructuredEngine:
         stream = torch.cuda.current_stream(self.dev)
         _lib.check(L.nlb_batch_launch(handle, ctypes_void(stream.cuda_stream)), "loop launch")
         b = b64 if b64 is not None else b32
-        c = self.read_ctrl(b)
-        self.last_fp32_ctrl = self.read_ctrl(b32) if (b32 is not None and b64 is not None) else \
-            (c if b32 is not None else None)
-        return c, b, self._loop_out.cpu().numpy()
+        return b, self._loop_out.cpu().numpy()   # one small read: energy, status, parity, counts
 
     # -- one phase of iterations ------------------------------------------
     def run(self, b, t1_init, t2c_init, e0, eps, mixing, max_steps, criterion, max_diis, ccs,
@@ -316,7 +314,7 @@ class StructuredEngine:
                         if stage == _lib.NLB_STAGE_T2:
                             ev1.record(stream)
                             t2_events.append((ev0, ev1))
-                self.launches += 5
+                self.launches += 4   # prep+Ga, T2, T1, finish
                 if use_diis and (done0 + k + 1) % max_diis == 0:
                     _lib.check(L.nlb_struct_diis(self.prob, st, max_diis, sp), "diis")
                     self.launches += 4
@@ -328,7 +326,7 @@ class StructuredEngine:
             if use_graph and n == chunk and b.get("warm"):
                 g = self._graph_for(b, chunk, max_diis if use_diis else 0, issue)
                 g.replay()
-                self.launches += (5 * chunk + (4 * (chunk // max_diis) if use_diis else 0))
+                self.launches += (4 * chunk + (4 * (chunk // max_diis) if use_diis else 0))
             else:
                 issue(n, done)
                 b["warm"] = True
@@ -361,6 +359,13 @@ def _issue_factory(eng, b, max_diis, stream):
 def ctypes_sizeof_ctrl():
     import ctypes
     return ctypes.sizeof(_lib.Ctrl)
+
+
+class _LoopResult:
+    """The parts of the control block a device-loop solve reports back."""
+
+    def __init__(self, parity, e_last, status):
+        self.parity, self.e_last, self.status = parity, e_last, status
 
 
 def _mp2_t1(f_pp, f_ph, f_hh, delta):
@@ -449,11 +454,16 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
     pl, dev = eng.plan, eng.dev
     crit = _CRIT[criterion]
     if t1initial is None:
-        t1 = _mp2_t1(eng.f_pp_np, eng.f_ph_np, eng.f_hh_np, float(delta))
+        # MP2 start, computed once per engine and delta and kept on the device
+        key = ("mp2", float(delta))
+        if key not in eng.cache:
+            t1 = _mp2_t1(eng.f_pp_np, eng.f_ph_np, eng.f_hh_np, float(delta))
+            eng.cache[key] = (torch.as_tensor(np.ascontiguousarray(t1), device=dev), float(np.sum(eng.f_ph_np * t1)))
+        t1_dev, e0 = eng.cache[key]
     else:
         t1 = np.asarray(_np(t1initial), dtype=np.float64)
-    e0 = float(np.sum(eng.f_ph_np * t1))
-    t1_dev = torch.as_tensor(np.ascontiguousarray(t1), device=dev)
+        e0 = float(np.sum(eng.f_ph_np * t1))
+        t1_dev = torch.as_tensor(np.ascontiguousarray(t1), device=dev)
     diis = int(max_diis) if crit == _lib.NLB_CRIT_SOA else 0
     sp = ctypes_void(torch.cuda.current_stream(dev).cuda_stream)
     iters = 0
@@ -469,15 +479,16 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
             phases = _lib.NLB_PHASE_FWD32 | (_lib.NLB_PHASE_FWD64 if refine else 0)
         else:
             phases = _lib.NLB_PHASE_FWD64
-        c, b, out = eng.device_loop(t1_dev, e0, phases, eps, me, mixing, maxSteps, crit, diis, chunk)
+        b, out = eng.device_loop(t1_dev, e0, phases, eps, me, mixing, maxSteps, crit, diis, chunk)
         iters = int(out[4])
-        # kernels run: five per step, four per DIIS pulse, the prologue and report
-        eng.launches += 5 * iters + (4 * (iters // diis) if diis else 0) + 3
+        # kernels run: four per step, four per DIIS pulse, the prologue and report
+        eng.launches += 4 * iters + (4 * (iters // diis) if diis else 0) + 3
         if precision == "mixed":
             info["mixed_iters"] = int(out[7])
-            info["mixed_energy"] = eng.last_fp32_ctrl.e_last
+            info["mixed_energy"] = float(out[2])
             if refine and phases & _lib.NLB_PHASE_FWD64:
                 info["refine_iters"] = iters - int(out[7])
+        c = _LoopResult(int(out[1]), float(out[0]), int(out[3]))
     elif precision == "mixed":
         b32 = eng.buffers(_lib.NLB_F32, diis)
         me = float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)

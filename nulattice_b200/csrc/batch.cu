@@ -133,12 +133,17 @@ __global__ void k_batch_gate(const nlb_ctrl* fwd, nlb_ctrl* lam) {
 // out[0] E_corr of the last forward phase, [3] its status, [4] forward
 // iterations (both phases), [5] Lambda status, [6] Lambda iterations (both
 // phases), [7] FP32 forward iterations; [1], [2] hold the coupling terms
-// (nlb_lambda_coupling).  Phases that did not run are passed as null.
+// (nlb_lambda_coupling), or without a Lambda phase the parity of the last
+// forward phase and the FP32 energy.  Phases that did not run are null.
 __global__ void k_batch_report(const nlb_ctrl* c32, const nlb_ctrl* c64, const nlb_ctrl* l32, const nlb_ctrl* l64,
                                double* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const nlb_ctrl* last = c64 ? c64 : c32;
     out[0] = last->e_last;
+    if (!l64) {   // forward only: the parity of the last phase and the FP32 energy
+        out[1] = (double)last->parity;
+        out[2] = c32 ? c32->e_last : last->e_last;
+    }
     out[3] = (double)last->status;
     out[4] = (double)((c32 ? c32->iter : 0) + (c64 ? c64->iter : 0));
     out[5] = l64 ? (double)l64->status : 0.0;

@@ -54,27 +54,28 @@ constexpr int kThreads = 256;
 #include "common.cuh"
 constexpr int kRowThreads = 256;   // T2 row kernel
 
-// ---------------------------------------------------------------- prep ----
-__global__ void k_prep(nlb_struct_problem P, nlb_struct_state S) {
-    const nlb_ctrl* c = S.ctrl;
-    if (c->status != NLB_RUNNING) return;
-    prep_body(P, S.t1[c->parity], S.prep, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
-}
-
-// ---------------------------------------------------------------- Ga ----
+// ----------------------------------------------------------- prep + Ga ----
 // Ga[k'][b'][i'j'] = sum_c f_ck B[c'][b'][i'j']  (k = hole k' of label g1):
 // the f_ph^T t2 half-contraction along the first particle index.  With t1 it
 // gives the rank-h part of X_pp t2 along a, and it holds the T1 Fock term
 // f_ck t2_acik for particles of label g2.
+// The dressed-Fock tables (from t1) and Ga (from t2) in one launch: they
+// read different amplitudes and are independent.
 template <typename T>
-__global__ void k_ga(nlb_struct_problem P, nlb_struct_state S) {
+__global__ void k_prep_ga(nlb_struct_problem P, nlb_struct_state S, int64_t nprep) {
     const nlb_ctrl* c = S.ctrl;
-    if (c->status != NLB_RUNNING || c->ccs) return;
+    if (c->status != NLB_RUNNING) return;
+    const double* t1 = S.t1[c->parity];
     const T* B = static_cast<const T*>(S.t2[c->parity]);
     T* G = static_cast<T*>(S.g);
+    const int64_t ng = (c->ccs || P.n_t2 == 0) ? 0 : P.n_g;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < P.n_g; e += stride) G[e] = ga_element(P, B, e);
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nprep + ng; u += stride) {
+        if (u < nprep) prep_body(P, t1, S.prep, u);
+        else G[u - nprep] = ga_element(P, B, u - nprep);
+    }
 }
+
 
 // --------------------------------------------------------- T2 update ----
 // One block per row task (channel, a').  The row B[a'][:][:] is staged in
@@ -601,6 +602,11 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
 // energy sum_ai f_ai t1'_ai (coupled_cluster.py:342-414, 265-286).
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nlb_struct_state S) {
+    // One warp per amplitude t1[a, i] of matching labels (the others are
+    // zero for label-conserving inputs and stay zero); the lanes share the
+    // terms of its residual: the T2 Fock terms of the channels holding the
+    // label (F2, or the Ga diagonal), the f_pp neighbours of a and the hole
+    // mixing over the label's holes.
     nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
     const int par = c->parity;
@@ -617,45 +623,56 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
     const int64_t n = (int64_t)p * h;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
-        const int a = (int)(idx / h), i = (int)(idx % h);
-        const int g = P.p_label[a];
-        if (P.h_label[i] != g) {
+        const int a = (int)(idx / h), i = (int)(idx - (int64_t)a * h);
+        if (P.h_label[i] != P.p_label[a]) {
             t1o[idx] = 0.0;
             if (E1) E1[idx] = 0.0;
-            continue;
         }
-        const int ap = P.p_loc[a], ip = P.h_loc[i];
-        double H1 = P.f_ph[idx];
+    }
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = stride >> 5;
+    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < P.n_t1c; q += nwarps) {
+        const int g = find_label(P.t1c_base, P.n_labels, q);
+        const int nh = P.h_base[g + 1] - P.h_base[g];
+        const int loc = (int)(q - P.t1c_base[g]);
+        const int ap = loc / nh, ip = loc - ap * nh;
+        const int pb = P.p_base[g];
+        const int a = P.p_ord[pb + ap], i = P.h_ord[P.h_base[g] + ip];
+        const int64_t idx = (int64_t)a * h + i;
+        double part = 0.0;
         if (!c->ccs) {
             for (int cc = 0; cc < P.n_channels; ++cc) {
                 const nlb_channel ch = P.chan[cc];
                 if (ch.g1 == g) {
-                    H1 += (double)F2[ch.f2_off + (int64_t)ap * ch.nh1 + ip];
-                } else if (ch.g2 == g) {
+                    if (lane == 0) part += (double)F2[ch.f2_off + (int64_t)ap * ch.nh1 + ip];
+                } else if (ch.g2 == g && lane < ch.nh1) {
                     const int nhp = ch.nh1 * ch.nh2;
                     const int64_t rowlen = (int64_t)ch.np2 * nhp;
-                    const T* g0 = Ga + ch.ga_off + (int64_t)ap * nhp + ip;
-                    for (int kq = 0; kq < ch.nh1; ++kq) H1 += (double)g0[kq * rowlen + kq * ch.nh2];
+                    part += (double)Ga[ch.ga_off + (int64_t)ap * nhp + ip + lane * rowlen + lane * ch.nh2];
                 }
             }
         }
-        const int pb = P.p_base[g];
         const int r = pb + ap;
-        for (int q = P.fpp_ptr[r]; q < P.fpp_ptr[r + 1]; ++q)
-            H1 += P.fpp_val[q] * t1[(int64_t)P.p_ord[pb + P.fpp_col[q]] * h + i];
-        for (int k = 0; k < h; ++k) {
-            const double tk = t1[(int64_t)a * h + k];
-            if (tk != 0.0) H1 += tk * (V.Xh1[(int64_t)k * h + i] - 0.5 * V.Q[(int64_t)k * h + i]);
+        const int q0 = P.fpp_ptr[r], q1 = P.fpp_ptr[r + 1];
+        for (int qq = q0 + lane; qq < q1; qq += 32)
+            part += P.fpp_val[qq] * t1[(int64_t)P.p_ord[pb + P.fpp_col[qq]] * h + i];
+        if (lane < nh) {
+            const int k = P.h_ord[P.h_base[g] + lane];
+            part += t1[(int64_t)a * h + k] * (V.Xh1[(int64_t)k * h + i] - 0.5 * V.Q[(int64_t)k * h + i]);
         }
-        const double D1 = -(V.dXp1[a] + V.Xh1[(int64_t)i * h + i]);
-        const double x = t1[idx];
-        const double tn = x + H1 / D1;
-        const double out = m * x + (1.0 - m) * tn;
-        t1o[idx] = out;
-        const double d = out - x;
-        if (E1) E1[idx] = d;
-        nrm += d * d;
-        eacc += P.f_ph[idx] * out;
+        part = warp_sum(part);
+        if (lane == 0) {
+            const double H1 = P.f_ph[idx] + part;
+            const double D1 = -(V.dXp1[a] + V.Xh1[(int64_t)i * h + i]);
+            const double x = t1[idx];
+            const double tn = x + H1 / D1;
+            const double out = m * x + (1.0 - m) * tn;
+            t1o[idx] = out;
+            const double d = out - x;
+            if (E1) E1[idx] = d;
+            nrm += d * d;
+            eacc += P.f_ph[idx] * out;
+        }
     }
     const double se = block_sum(eacc);
     const double sn = block_sum(nrm);
@@ -1040,12 +1057,13 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
     switch (stage) {
         case NLB_STAGE_PREP: {
             const int64_t nprep = (int64_t)P->h * P->h + 2 * (int64_t)P->p + P->n_t1c + P->n_xc + P->h;
-            k_prep<<<(unsigned)((nprep + kThreads - 1) / kThreads), kThreads, 0, st>>>(*P, *S);
+            // the dressed-Fock tables and Ga in one launch (the GTERMS stage is then empty)
+            const int64_t ng = P->n_t2 > 0 ? P->n_g : 0;
+            k_prep_ga<T><<<grid_for(k_prep_ga<T>, nprep + ng), kThreads, 0, st>>>(*P, *S, nprep);
             break;
         }
         case NLB_STAGE_GTERMS:
-            if (P->n_t2 > 0) k_ga<T><<<grid_for(k_ga<T>, P->n_g), kThreads, 0, st>>>(*P, *S);
-            break;
+            break;   // Ga is formed with the prep tables
         case NLB_STAGE_T2:
             if (P->n_t2 > 0 && use_lat(P, sizeof(T))) {
                 // launch shape from the problem's tuning word (FP32: bits 0-3, FP64:
@@ -1070,7 +1088,7 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
             }
             break;
         case NLB_STAGE_T1:
-            k_t1_update<T><<<grid_for(k_t1_update<T>, (int64_t)P->p * P->h), kThreads, 0, st>>>(*P, *S);
+            k_t1_update<T><<<grid_for(k_t1_update<T>, 32 * (int64_t)P->n_t1c), kThreads, 0, st>>>(*P, *S);
             break;
         default:
             k_finish<<<1, 32, 0, st>>>(S->ctrl);
