@@ -222,8 +222,10 @@ def main():
         return e, info
 
     if args.profile:
+        # stage by stage (t2_events): kernels inside the device-loop graph are
+        # not seen by a kernel profiler
         C.solve_structured(eng, eps=0.0, maxSteps=12, max_diis=8, precision="mixed", mixed_eps=0.0,
-                           t2_format="compact")
+                           t2_format="compact", t2_events=[])
         torch.cuda.synchronize()
         print("profile run done", flush=True)
         return
@@ -316,7 +318,9 @@ def main():
     tfile = os.path.join(ROOT, "profiles", "t2_update_traffic.json")
     if os.path.exists(tfile):
         traffic = json.load(open(tfile)).get("bytes_per_launch")
-    roofline = {"kernel": "k_t2_lat<float, 7, 256, 2>", "bound": "hbm", "achieved": achieved, "peak": peak,
+    shape = T.describe(int(eng.prob.tune))["t2_fp32"] or "256x2"
+    nt_, mb_ = shape.split("x")
+    roofline = {"kernel": f"k_t2_lat<float, 7, {nt_}, {mb_}>", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_us": k_ms * 1e3, "launches": len(m_k)}
 

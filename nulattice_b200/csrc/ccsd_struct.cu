@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_t2_rows(nlb_struct_problem P
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int64_t task = blockIdx.x; task < P.n_rows; task += gridDim.x) {
         const int ci = find_seg(P.row_end, P.n_channels, task);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
         const int nh1 = NH ? NH : ch.nh1, nh2 = NH ? NH : ch.nh2, np2 = ch.np2;
         const int nhp = nh1 * nh2;
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
     }
     for (int64_t task = t0; task < t1e; ++task) {
         const int buf = (int)((task - t0) & 1);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
         const int np2 = ch.np2;
         const int rowlen = np2 * NHP;
@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
         double part = 0.0;
         if (!c->ccs) {
             for (int cc = 0; cc < P.n_channels; ++cc) {
-                const nlb_channel ch = P.chan[cc];
+                const nlb_channel& ch = P.chan[cc];
                 if (ch.g1 == g) {
                     if (lane == 0) part += (double)F2[ch.f2_off + (int64_t)ap * ch.nh1 + ip];
                 } else if (ch.g2 == g && lane < ch.nh1) {
@@ -924,7 +924,7 @@ __global__ void k_unpack(nlb_struct_problem P, const T* t2c, double* t2) {
     const int64_t p = P.p, h = P.h;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < P.n_t2; e += (int64_t)gridDim.x * blockDim.x) {
         const int ci = find_seg(P.t2_end, P.n_channels, e);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int64_t loc = e - ch.offset;
         const int nhp = ch.nh1 * ch.nh2;
         const int hp = (int)(loc % nhp);
@@ -944,7 +944,7 @@ __global__ void k_pack(nlb_struct_problem P, const double* t2, T* t2c) {
     const int64_t p = P.p, h = P.h;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < P.n_t2; e += (int64_t)gridDim.x * blockDim.x) {
         const int ci = find_seg(P.t2_end, P.n_channels, e);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int64_t loc = e - ch.offset;
         const int nhp = ch.nh1 * ch.nh2;
         const int hp = (int)(loc % nhp);

@@ -145,7 +145,7 @@ __device__ void prep_body(const nlb_struct_problem& P, const double* t1, double*
 template <typename T>
 __device__ __forceinline__ T ga_element(const nlb_struct_problem& P, const T* B, int64_t e) {
     const int ci = find_seg(P.g_end, P.n_channels, e);
-    const nlb_channel ch = P.chan[ci];
+    const nlb_channel& ch = P.chan[ci];
     const int rowlen = ch.np2 * ch.nh1 * ch.nh2;
     const int loc = (int)(e - ch.ga_off);
     const int kq = loc / rowlen, rem = loc - kq * rowlen;

@@ -103,7 +103,7 @@ __global__ void k_l_ha(nlb_struct_problem P, nlb_lambda_state S) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_g; u += stride) {
         const int ci = find_seg(P.g_end, P.n_channels, u);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int rowlen = ch.np2 * ch.nh1 * ch.nh2;
         const int loc = (int)(u - ch.ga_off);
         const int kq = loc / rowlen, e = loc - kq * rowlen;
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int64_t task = blockIdx.x; task < P.n_rows; task += gridDim.x) {
         const int ci = find_seg(P.row_end, P.n_channels, task);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
         const int nh1 = ch.nh1, nh2 = ch.nh2, np2 = ch.np2;
         const int nhp = nh1 * nh2;
@@ -406,7 +406,7 @@ __global__ void k_l_coupling(nlb_struct_problem P, nlb_lambda_state S, const dou
     double acc = 0.0;
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_t2; u += (int64_t)gridDim.x * blockDim.x) {
         const int ci = find_seg(P.t2_end, P.n_channels, u);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int64_t loc = u - ch.offset;
         const int nhp = ch.nh1 * ch.nh2;
         const int hp = (int)(loc % nhp);
@@ -454,7 +454,7 @@ __global__ void k_l_setup_lat(nlb_struct_problem P, nlb_lambda_state S) {
             const int rem = (int)(v - task * (kLH * kLHP));
             const int kq = rem / kLHP, hp = rem - kq * kLHP;
             const int ci = find_seg(P.row_end, P.n_channels, task);
-            const nlb_channel ch = P.chan[ci];
+            const nlb_channel& ch = P.chan[ci];
             const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
             const int64_t rowlen = (int64_t)ch.np2 * kLHP;
             const T* Brow = t2 + ch.offset + ap * rowlen;
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lamb
         item -= nit;
     }
     if (ci >= P.n_channels) return;   // uniform over the block
-    const nlb_channel ch = P.chan[ci];
+    const nlb_channel& ch = P.chan[ci];
     const int bb = (int)(item / nchunk), chunk = (int)(item - (int64_t)bb * nchunk);
     const int a0 = (int)((int64_t)chunk * ch.np1 / nchunk), a1 = (int)((int64_t)(chunk + 1) * ch.np1 / nchunk);
     const int bp = bb * NB + grp;
@@ -687,7 +687,7 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
     const int64_t t1e = (int64_t)(blockIdx.x + 1) * P.n_rows / gridDim.x;
     for (int64_t task = t0; task < t1e; ++task) {
         const int ci = find_seg(P.row_end, P.n_channels, task);
-        const nlb_channel ch = P.chan[ci];
+        const nlb_channel& ch = P.chan[ci];
         const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
         const int np2 = ch.np2;
         const int rowlen = np2 * kLHP;
