@@ -45,6 +45,28 @@ def draw_instances(n=64, seed=0):
     return out
 
 
+def instance_cost(A, L):
+    """Compact T2 length of a closed-shell instance: four labels, A/4 holes and
+    L^3 - A/4 particles per label, six label-pair channels."""
+    nh = A // 4
+    npl = L ** 3 - nh
+    return 6 * npl * npl * nh * nh
+
+
+def shard(instances, rank, world):
+    """The instances rank `rank` of `world` GPUs solves: largest first onto the
+    least-loaded rank (by compact T2 size), deterministic, disjoint, together
+    all of them.  The batch needs no communication between ranks."""
+    load = [0] * world
+    owner = {}
+    order = sorted(range(len(instances)), key=lambda i: (-instance_cost(instances[i][0], instances[i][1]), i))
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += instance_cost(instances[i][0], instances[i][1])
+    return [instances[i] for i in range(len(instances)) if owner[i] == rank]
+
+
 def combine(parts, coeffs):
     """sum_k c_k H_k of builder outputs (E_ref, fock, two-body blocks); sparse
     blocks are concatenated (repeated keys are summed downstream)."""

@@ -162,3 +162,16 @@ def test_batch_hamiltonian_is_the_builder_output():
         oa, ob = np.lexsort(ia.T[::-1]), np.lexsort(ib.T[::-1])
         np.testing.assert_array_equal(ia[oa], ib[ob])
         np.testing.assert_allclose(va[oa], vb[ob], atol=1e-13)
+
+
+def test_batch_shards_are_disjoint_complete_and_balanced():
+    from nulattice_b200 import batch as B
+    inst = B.draw_instances(64, 0)
+    for world in (1, 2, 4, 8):
+        parts = [B.shard(inst, r, world) for r in range(world)]
+        got = sorted(x for p in parts for x in p)
+        assert got == sorted(inst)
+        loads = [sum(B.instance_cost(a, l) for a, l, _, _ in p) for p in parts]
+        biggest = max(B.instance_cost(a, l) for a, l, _, _ in inst)
+        assert max(loads) - min(loads) <= biggest
+    assert B.instance_cost(28, 6) == 6 * 209 * 209 * 49
