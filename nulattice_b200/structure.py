@@ -73,32 +73,38 @@ def _to_np(x):
 
 
 def _components(n, edges):
-    parent = np.arange(n)
-
-    def find(x):
-        while parent[x] != x:
-            parent[x] = parent[parent[x]]
-            x = parent[x]
-        return x
-
-    for a, b in edges:
-        ra, rb = find(a), find(b)
-        if ra != rb:
-            parent[max(ra, rb)] = min(ra, rb)
-    roots = np.array([find(i) for i in range(n)])
-    _, lab = np.unique(roots, return_inverse=True)
-    return lab.astype(np.int64)
+    """Connected-component label (0..k-1, ordered by smallest member) of each
+    of n vertices."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    e = np.asarray(list(edges), dtype=np.int64).reshape(-1, 2)
+    g = coo_matrix((np.ones(len(e)), (e[:, 0], e[:, 1])), shape=(n, n))
+    _, lab = connected_components(g, directed=False)
+    # relabel by the smallest member, as a union-find with min roots would
+    first = np.full(lab.max() + 1 if n else 0, n, dtype=np.int64)
+    np.minimum.at(first, lab, np.arange(n))
+    _, out = np.unique(first[lab], return_inverse=True)
+    return out.astype(np.int64)
 
 
 def _antisym_ok(idx, val, n0, n1, tol=0.0):
-    """True when v[a,b,c,d] = -v[b,a,c,d] = -v[a,b,d,c] entry by entry."""
+    """True when v[a,b,c,d] = -v[b,a,c,d] = -v[a,b,d,c] entry by entry
+    (idx unique; entries absent from the list are zero)."""
     if len(val) == 0:
         return True
-    d = {tuple(r): v for r, v in zip(idx.tolist(), val.tolist())}
-    for (a, b, c, e), v in d.items():
-        if abs(d.get((b, a, c, e), 0.0) + v) > tol * abs(v):
-            return False
-        if abs(d.get((a, b, e, c), 0.0) + v) > tol * abs(v):
+    idx = np.asarray(idx, dtype=np.int64)
+    val = np.asarray(val, dtype=np.float64)
+    dims = idx.max(axis=0) + 1
+    size = int(max(dims[0], dims[1])) , int(max(dims[2], dims[3]))
+    key = lambda a, b, c, d: ((a * size[0] + b) * size[1] + c) * size[1] + d  # noqa: E731
+    k0 = key(idx[:, 0], idx[:, 1], idx[:, 2], idx[:, 3])
+    order = np.argsort(k0)
+    ks, vs = k0[order], val[order]
+    for k in (key(idx[:, 1], idx[:, 0], idx[:, 2], idx[:, 3]), key(idx[:, 0], idx[:, 1], idx[:, 3], idx[:, 2])):
+        pos = np.searchsorted(ks, k)
+        pos = np.minimum(pos, len(ks) - 1)
+        partner = np.where(ks[pos] == k, vs[pos], 0.0)
+        if np.any(np.abs(partner + val) > tol * np.abs(val)):
             return False
     return True
 
