@@ -524,7 +524,7 @@ def e2e_leg(args, fock, two, dev):
     from nulattice_b200 import ccsd_solver
     h2d = sum(np.asarray(f).nbytes for f in fock) + sum(
         (b.indices.nbytes + b.values.nbytes) if hasattr(b, "indices") else np.asarray(b).nbytes for b in two)
-    times = []
+    times, phases = [], {}
     for k in range(args.warmup + args.steps):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
@@ -537,9 +537,14 @@ def e2e_leg(args, fock, two, dev):
         torch.cuda.synchronize()
         if k >= args.warmup:
             times.append(a.elapsed_time(b) / 1e3)
+            for name in ("t_detect", "t_engine", "t_solve", "t_output"):
+                phases.setdefault(name, []).append(info.get(name, 0.0))
     d2h = 8 + t1.nbytes + t2.nbytes
     return {"value": statistics.mean(times), "unit": "s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "iterations": info.get("iterations")}
+            "d2h_bytes_per_step": int(d2h), "iterations": info.get("iterations"),
+            "phases_ms": {k: round(statistics.mean(v) * 1e3, 3) for k, v in phases.items()},
+            "path": "ccsd_solver(numpy inputs): structure detection, engine build, eager mixed solve, "
+                    "E/t1/compact-t2 to host (page-locked)"}
 
 
 if __name__ == "__main__":

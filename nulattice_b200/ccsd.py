@@ -247,6 +247,7 @@ class StructuredEngine:
         b32 = self.buffers(_lib.NLB_F32, max_diis) if phases & _lib.NLB_PHASE_FWD32 else None
         b64 = self.buffers(_lib.NLB_F64, max_diis) if phases & _lib.NLB_PHASE_FWD64 else None
         if key not in self._loops:
+            t_build = time.perf_counter()
             it = _lib.BatchItem()
             it.prob = ctypes.pointer(self.prob)
             if b32 is not None:
@@ -263,6 +264,7 @@ class StructuredEngine:
             handle = ctypes.c_void_p()
             _lib.check(L.nlb_batch_create(items, 1, ctypes.byref(cfg), ctypes.byref(handle)), "loop create")
             self._loops[key] = (handle, items)
+            self.cache["t_loop_build"] = time.perf_counter() - t_build
         handle = self._loops[key][0]
         self._loop_t1.copy_(t1_init.reshape(-1))
         stream = torch.cuda.current_stream(self.dev)
@@ -368,6 +370,18 @@ class _LoopResult:
         self.parity, self.e_last, self.status = parity, e_last, status
 
 
+def _to_host(t):
+    """Device tensor -> numpy array.  Large results land in page-locked
+    memory from torch's host cache (a copy at PCIe speed, and the block is
+    reused by the next call once the array is freed); small ones take the
+    plain pageable copy."""
+    if t.device.type != "cuda" or t.numel() * t.element_size() < (1 << 20):
+        return t.cpu().numpy()
+    out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    out.copy_(t)
+    return out.numpy()
+
+
 def _mp2_t1(f_pp, f_ph, f_hh, delta):
     """``t1Init`` (``CCM/coupled_cluster.py:319-340``)."""
     den = np.add.outer(-np.diag(f_pp), np.diag(f_hh)) + delta
@@ -378,7 +392,7 @@ def _mp2_t1(f_pp, f_ph, f_hh, delta):
 def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10,
                 delta=0, mixing=0.5, verbose=False, sparse=True, ccs=False, device=None,
                 dtype=torch.float64, *, precision="fp64", criterion="soa", t2_format="dense",
-                mixed_eps=None, info=None, engine="auto"):
+                mixed_eps=None, info=None, engine="auto", loop="eager"):
     """Solve the CCSD equations; returns ``(E_corr, t1, t2)``.
 
     Arguments as ``CCM/soa/coupled_cluster.py:440-454``: ``fock_mats`` =
@@ -393,6 +407,11 @@ def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000
     arrays otherwise.  On divergence the last amplitudes are returned (the
     NumPy reference returns None there) and ``info["status"]`` says
     ``"diverged"``.
+
+    ``loop``: "eager" (default: every call builds a fresh engine, so a solve
+    graph would be built for one use) or "graph" (the whole solve as one
+    graph launch with device-side loops).  ``info`` receives the time of each
+    phase: ``t_detect``, ``t_engine``, ``t_solve``, ``t_output``.
     """
     t_start = time.perf_counter()
     dev = _resolve_device(device)
@@ -411,12 +430,16 @@ def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000
     if engine == "general":
         plan, why = None, "general engine requested"
     else:
+        t_detect = time.perf_counter()
         plan, why = _structure.detect(fock_mats, two_body_int, t1initial)
+        t_detect = time.perf_counter() - t_detect
         if plan is None and engine == "structured":
             raise ValueError(f"structured engine does not apply: {why}")
     if info is None:
         info = {}
     info["t_setup_start"] = t_start
+    if engine != "general":
+        info["t_detect"] = t_detect
     if plan is None:
         from . import dense as _dense
         info["engine"] = "general"
@@ -426,11 +449,16 @@ def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000
                                  device=dev, criterion=criterion, info=info)
     else:
         info["engine"] = "structured"
+        t0 = time.perf_counter()
         eng = StructuredEngine(plan, fock_mats, dev)
+        info["t_engine"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
         e, t1, t2 = solve_structured(eng, t1initial=t1initial, eps=eps, maxSteps=maxSteps,
                                      max_diis=max_diis, delta=delta, mixing=mixing, verbose=verbose,
                                      ccs=ccs, criterion=criterion, precision=precision,
-                                     t2_format=t2_format, mixed_eps=mixed_eps, info=info)
+                                     t2_format=t2_format, mixed_eps=mixed_eps, info=info, loop=loop)
+        info["t_solve"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
     if info.get("status") == "max_iter":
         print("Max iterations reached.")
     elif info.get("status") == "diverged":
@@ -439,16 +467,22 @@ def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000
         t1 = t1.to(dtype)
         t2 = t2.to(dtype) if t2 is not None else t2
     else:
-        t1 = t1.cpu().numpy()
-        t2 = t2.cpu().numpy() if t2 is not None else t2
+        t1 = _to_host(t1)
+        t2 = _to_host(t2) if t2 is not None else t2
+    info["t_output"] = time.perf_counter() - t0
     info["t_total"] = time.perf_counter() - t_start
     return e, t1, t2
 
 
 def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5,
                      verbose=False, ccs=False, criterion="soa", precision="fp64", t2_format="dense",
-                     mixed_eps=None, info=None, sync_every=16, t2_events=None, refine=True):
-    """Run the structured engine (already built); see :func:`ccsd_solver`."""
+                     mixed_eps=None, info=None, sync_every=16, t2_events=None, refine=True, loop="graph"):
+    """Run the structured engine (already built); see :func:`ccsd_solver`.
+
+    ``loop``: "graph" runs the whole solve as one graph launch with
+    device-side loops (the graph is built on the first solve of an engine and
+    replayed by later ones); "eager" launches the steps chunk by chunk from
+    the host, which costs no graph build and suits an engine used once."""
     info = {} if info is None else info
     L = _lib.lib()
     pl, dev = eng.plan, eng.dev
@@ -468,7 +502,9 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
     sp = ctypes_void(torch.cuda.current_stream(dev).cuda_stream)
     iters = 0
     t0 = time.perf_counter()
-    if t2_events is None and not verbose and not ccs:
+    if loop not in ("graph", "eager"):
+        raise ValueError("loop must be 'graph' or 'eager'")
+    if loop == "graph" and t2_events is None and not verbose and not ccs:
         # the whole solve as one graph launch: device-side loops, no host
         # round trip per chunk of steps
         chunk = diis if diis else sync_every
@@ -479,7 +515,10 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
             phases = _lib.NLB_PHASE_FWD32 | (_lib.NLB_PHASE_FWD64 if refine else 0)
         else:
             phases = _lib.NLB_PHASE_FWD64
+        eng.cache.pop("t_loop_build", None)
         b, out = eng.device_loop(t1_dev, e0, phases, eps, me, mixing, maxSteps, crit, diis, chunk)
+        if "t_loop_build" in eng.cache:
+            info["t_loop_build"] = eng.cache["t_loop_build"]
         iters = int(out[4])
         # kernels run: four per step, four per DIIS pulse, the prologue and report
         eng.launches += 4 * iters + (4 * (iters // diis) if diis else 0) + 3
@@ -493,7 +532,7 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
         b32 = eng.buffers(_lib.NLB_F32, diis)
         me = float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)
         c = eng.run(b32, t1_dev, None, e0, me, mixing, maxSteps, crit, diis, ccs, verbose, sync_every,
-                    t2_events=t2_events)
+                    t2_events=t2_events, graph=loop == "graph")
         iters += c.iter
         info["mixed_iters"] = c.iter
         info["mixed_energy"] = c.e_last
@@ -505,7 +544,7 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
             _lib.check(L.nlb_convert(b32["t2"][cur].data_ptr(), _lib.NLB_F32, b64["t2"][0].data_ptr(),
                                      _lib.NLB_F64, pl.n_t2, sp), "convert")
             c = eng.run(b64, b32["t1"][cur].clone(), b64["t2"][0], c.e_last, eps, mixing, maxSteps - iters,
-                        crit, diis, ccs, verbose, sync_every, step_offset=iters)
+                        crit, diis, ccs, verbose, sync_every, step_offset=iters, graph=loop == "graph")
             eng.launches += 1
             iters += c.iter
             info["refine_iters"] = c.iter
@@ -515,7 +554,7 @@ def solve_structured(eng, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, 
     else:
         b = eng.buffers(_lib.NLB_F64, diis)
         c = eng.run(b, t1_dev, None, e0, eps, mixing, maxSteps, crit, diis, ccs, verbose, sync_every,
-                    t2_events=t2_events)
+                    t2_events=t2_events, graph=loop == "graph")
         iters += c.iter
     torch.cuda.current_stream(dev).synchronize()
     info["t_iterate"] = time.perf_counter() - t0

@@ -59,9 +59,20 @@ def _coo(block):
     idx = idx.reshape(-1, 4)
     if len(val) == 0:
         return idx, val
-    uniq, inv = np.unique(idx, axis=0, return_inverse=True)
-    acc = np.zeros(len(uniq))
-    np.add.at(acc, inv.reshape(-1), val)
+    dims = idx.max(axis=0) + 1
+    if idx.min() < 0 or float(np.prod(dims.astype(np.float64))) >= 2.0 ** 62:
+        uniq, inv = np.unique(idx, axis=0, return_inverse=True)
+        acc = np.zeros(len(uniq))
+        np.add.at(acc, inv.reshape(-1), val)
+        keep = acc != 0
+        return uniq[keep], acc[keep]
+    # rows sorted lexicographically = sorted by the mixed-radix key
+    key = ((idx[:, 0] * dims[1] + idx[:, 1]) * dims[2] + idx[:, 2]) * dims[3] + idx[:, 3]
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    start = np.flatnonzero(np.concatenate(([True], ks[1:] != ks[:-1])))
+    acc = np.add.reduceat(val[order], start)
+    uniq = idx[order[start]]
     keep = acc != 0
     return uniq[keep], acc[keep]
 
@@ -72,13 +83,13 @@ def _to_np(x):
     return x
 
 
-def _components(n, edges):
+def _components(n, src, dst):
     """Connected-component label (0..k-1, ordered by smallest member) of each
-    of n vertices."""
+    of n vertices joined by the edges (src[k], dst[k])."""
     from scipy.sparse import coo_matrix
     from scipy.sparse.csgraph import connected_components
-    e = np.asarray(list(edges), dtype=np.int64).reshape(-1, 2)
-    g = coo_matrix((np.ones(len(e)), (e[:, 0], e[:, 1])), shape=(n, n))
+    src = np.asarray(src, dtype=np.int64)
+    g = coo_matrix((np.ones(len(src)), (src, np.asarray(dst, dtype=np.int64))), shape=(n, n))
     _, lab = connected_components(g, directed=False)
     # relabel by the smallest member, as a union-find with min roots would
     first = np.full(lab.max() + 1 if n else 0, n, dtype=np.int64)
@@ -198,12 +209,11 @@ def detect(fock_mats, two_body_int, t1initial=None):
         if len(_coo(blk)[1]):
             return None, f"{name} is non-zero (open-shell site or non-conserving contact)"
     n = p + h
-    ip = np.argwhere(f_pp != 0)
-    ih = np.argwhere(f_ph != 0)
-    ihh = np.argwhere(f_hh != 0)
-    edges = [(int(a), int(b)) for a, b in ip] + [(int(a), p + int(i)) for a, i in ih] + \
-            [(p + int(i), p + int(j)) for i, j in ihh]
-    lab = _components(n, edges)
+    fpp_r, fpp_c = np.nonzero(f_pp)
+    fph_r, fph_c = np.nonzero(f_ph)
+    fhh_r, fhh_c = np.nonzero(f_hh)
+    lab = _components(n, np.concatenate([fpp_r, fph_r, p + fhh_r]),
+                      np.concatenate([fpp_c, p + fph_c, p + fhh_c]))
     G = int(lab.max()) + 1 if n else 0
     if G < 2:
         return None, "one-body part connects every state (no conserved label)"
@@ -245,24 +255,27 @@ def detect(fock_mats, two_body_int, t1initial=None):
             channels.append(ch)
             off += ch.size
 
-    # f_pp CSR (label-ordered rows, label-local columns)
-    ptr, col, val = [0], [], []
-    for g in range(G):
-        P = p_of[g]
-        sub = f_pp[np.ix_(P, P)]
-        for r in range(len(P)):
-            nz = np.flatnonzero(sub[r])
-            col += nz.tolist(); val += sub[r, nz].tolist(); ptr.append(len(col))
-    fpp_ptr, fpp_col, fpp_val = np.array(ptr, np.int64), np.array(col, np.int64), np.array(val)
-    # f_ph per hole
-    ptr, col, val = [0], [], []
-    for g in range(G):
-        P, Hh = p_of[g], h_of[g]
-        sub = f_ph[np.ix_(P, Hh)]
-        for k in range(len(Hh)):
-            nz = np.flatnonzero(sub[:, k])
-            col += nz.tolist(); val += sub[nz, k].tolist(); ptr.append(len(col))
-    fph_ptr, fph_col, fph_val = np.array(ptr, np.int64), np.array(col, np.int64), np.array(val)
+    # f_pp CSR (label-ordered rows, label-local columns).  Every non-zero of
+    # f_pp joins two states of one label, so in label order the matrix is
+    # block diagonal and a column's local index is its position minus the
+    # label's base.
+    p_ord = np.concatenate(p_of) if G else np.zeros(0, np.int64)
+    h_ord = np.concatenate(h_of) if G else np.zeros(0, np.int64)
+    p_pos = np.empty(p, np.int64); p_pos[p_ord] = np.arange(p)
+    h_pos = np.empty(h, np.int64); h_pos[h_ord] = np.arange(h)
+    r, c = p_pos[fpp_r], p_pos[fpp_c]
+    order = np.argsort(r * max(p, 1) + c, kind="stable")
+    r, c = r[order], c[order]
+    fpp_ptr = np.concatenate(([0], np.cumsum(np.bincount(r, minlength=p)))).astype(np.int64)
+    fpp_col = (c - p_base[p_label[p_ord[c]]]).astype(np.int64)
+    fpp_val = np.ascontiguousarray(f_pp[fpp_r[order], fpp_c[order]], dtype=np.float64)
+    # f_ph per hole (label-ordered holes, label-local particle rows)
+    r, c = h_pos[fph_c], p_pos[fph_r]
+    order = np.argsort(r * max(p, 1) + c, kind="stable")
+    r, c = r[order], c[order]
+    fph_ptr = np.concatenate(([0], np.cumsum(np.bincount(r, minlength=h)))).astype(np.int64)
+    fph_col = (c - p_base[p_label[p_ord[c]]]).astype(np.int64)
+    fph_val = np.ascontiguousarray(f_ph[fph_r[order], fph_c[order]], dtype=np.float64)
 
     # ladders per channel
     hh_ptr, hh_col, hh_val, pp_ptr, pp_col, pp_val = [], [], [], [], [], []
@@ -277,7 +290,7 @@ def detect(fock_mats, two_body_int, t1initial=None):
         else:
             out = inp = np.zeros(0, np.int64); vv = np.zeros(0)
         order = np.argsort(out, kind="stable")
-        hh_ptr.append(np.searchsorted(out[order], np.arange(ch.nh1 * ch.nh2 + 1)).astype(np.int64))
+        hh_ptr.append(np.concatenate(([0], np.cumsum(np.bincount(out, minlength=ch.nh1 * ch.nh2)))).astype(np.int64))
         hh_col.append(inp[order].astype(np.int64)); hh_val.append(vv[order])
         # particle-particle: output (a,b) in (g1,g2), input (c,d) in (g1,g2)
         if len(pp_idx):
@@ -289,7 +302,7 @@ def detect(fock_mats, two_body_int, t1initial=None):
         else:
             out = inp = np.zeros(0, np.int64); vv = np.zeros(0)
         order = np.argsort(out, kind="stable")
-        pp_ptr.append(np.searchsorted(out[order], np.arange(ch.np1 * ch.np2 + 1)).astype(np.int64))
+        pp_ptr.append(np.concatenate(([0], np.cumsum(np.bincount(out, minlength=ch.np1 * ch.np2)))).astype(np.int64))
         pp_col.append(inp[order].astype(np.int64)); pp_val.append(vv[order])
 
     plan = ChannelPlan(p=p, h=h, n_labels=G, p_label=p_label, h_label=h_label, p_loc=p_loc,
