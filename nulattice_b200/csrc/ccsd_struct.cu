@@ -338,8 +338,9 @@ struct LatSmem {
     int64_t row0, row1, gb, rec, dp, off, val, total;
 };
 
-// Shared-memory layout of k_t2_lat for element size el and NH holes per label.
-__host__ __device__ inline LatSmem lat_smem(int64_t max_row, int nh, int64_t el) {
+// Shared-memory layout of k_t2_lat for element size el and NH holes per label
+// (pair: the per-b' record holds 8 (f_pp value, t1) pairs instead of 8 t1).
+__host__ __device__ inline LatSmem lat_smem(int64_t max_row, int nh, int64_t el, bool pair = false) {
     const int64_t np2 = max_row / (nh * nh);
     const int64_t rowb = lat_round16(el * (max_row + 16 / el + 4));
     LatSmem s;
@@ -347,7 +348,7 @@ __host__ __device__ inline LatSmem lat_smem(int64_t max_row, int nh, int64_t el)
     s.row1 = rowb;
     s.gb = 2 * rowb;
     s.rec = s.gb + lat_round16(el * nh * nh * nh);
-    s.dp = s.rec + lat_round16(el * np2 * kLatNb);
+    s.dp = s.rec + lat_round16(el * np2 * kLatNb * (pair ? 2 : 1));
     s.off = s.dp + lat_round16(el * np2);
     s.val = s.off + lat_round16(4 * np2 * kLatNb);
     s.total = s.val + lat_round16(el * np2 * kLatNb);
@@ -372,8 +373,14 @@ __device__ __forceinline__ int lat_issue_row(T* dst, const T* src, int rowlen) {
     return mis;
 }
 
-template <typename T, int NH, int NT, int MINB>
+//
+// PAIR (FP32 only): the three pairs of independent sums (along b / rank-h
+// along b, X_hh along i / along j, along a / rank-h along a) run as packed
+// FP32x2 fused multiply-adds, with the f_pp values and t1 of b' interleaved
+// in the per-b' record so that each coefficient pair is one register pair.
+template <typename T, int NH, int NT, int MINB, bool PAIR = false>
 __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_struct_state S) {
+    static_assert(!PAIR || sizeof(T) == 4, "packed pairs are FP32x2");
     constexpr int NHP = NH * NH;
     constexpr int NB = NT / NHP;
     static_assert(NB >= 1 && NH <= 7, "block must hold one hole-pair group; a record holds 7 holes");
@@ -389,9 +396,12 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
     T* E2 = (S.diis_t2 != nullptr && c->max_diis > 0 && c->diis_count < c->max_diis)
                 ? static_cast<T*>(S.diis_t2) + (int64_t)c->diis_count * P.n_t2 : nullptr;
     const T m = (T)c->mixing, om = (T)(1.0 - c->mixing);
-    const LatSmem L = lat_smem(P.max_row, NH, sizeof(T));
+    const LatSmem L = lat_smem(P.max_row, NH, sizeof(T), PAIR);
     T* sgb = reinterpret_cast<T*>(smem_raw + L.gb);        // Gb[k'][i'j'] of this row
-    T* srec = reinterpret_cast<T*>(smem_raw + L.rec);      // [b'][8]: t1[b', k'] (k' < NH), pp ladder at 7
+    // [b'][8]: t1[b', k'] (k' < NH), pp ladder at 7; PAIR: [b'][8][2] (f_pp value, t1[b', k']),
+    // pp ladder at [7][1]
+    T* srec = reinterpret_cast<T*>(smem_raw + L.rec);
+    constexpr int RW = PAIR ? 2 * kLatNb : kLatNb;         // record width
     T* sdp = reinterpret_cast<T*>(smem_raw + L.dp);        // [b']: particle part of the denominator
     int32_t* soff = reinterpret_cast<int32_t*>(smem_raw + L.off);   // [b'][8] f_pp columns * NH^2
     T* sval = reinterpret_cast<T*>(smem_raw + L.val);      // [b'][8] f_pp values (0 = padding)
@@ -403,6 +413,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
     double nrm = 0.0;
     int cur_ci = -1;
     T x1[NH], x2[NH], hh = T(0), dh = T(0);
+    float2 x12[NH];   // PAIR: (x1[k], x2[k])
 
     const int64_t t0 = (int64_t)blockIdx.x * P.n_rows / gridDim.x;
     const int64_t t1e = (int64_t)(blockIdx.x + 1) * P.n_rows / gridDim.x;
@@ -433,6 +444,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
             for (int k = 0; k < NH; ++k) {
                 x1[k] = (T)V.xc[x1b + k * NH + ip];
                 x2[k] = (T)V.xc[x2b + k * NH + jp];
+                x12[k] = make_float2((float)x1[k], (float)x2[k]);
             }
             const int32_t* hptr = P.hh_ptr + ch.hh_ptr_off;
             hh = (hptr[hp + 1] > hptr[hp]) ? (T)P.hh_val[ch.hh_col_off + hptr[hp]] : T(0);
@@ -440,10 +452,16 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
             const int t1b_b = P.t1c_base[ch.g2];
             for (int w = tid; w < np2 * kLatNb; w += NT) {
                 const int bp = w / kLatNb, k = w - bp * kLatNb;
-                if (k < NH) srec[w] = (T)V.t1c[t1b_b + bp * NH + k];
                 const int r0 = P.fpp_ptr[ch.pb2 + bp], r1 = P.fpp_ptr[ch.pb2 + bp + 1];
                 soff[w] = ((k < r1 - r0) ? P.fpp_col[r0 + k] : bp) * NHP;
-                sval[w] = (k < r1 - r0) ? (T)P.fpp_val[r0 + k] : T(0);
+                const T v = (k < r1 - r0) ? (T)P.fpp_val[r0 + k] : T(0);
+                if constexpr (PAIR) {
+                    srec[2 * w] = v;
+                    if (k < NH) srec[2 * w + 1] = (T)V.t1c[t1b_b + bp * NH + k];
+                } else {
+                    if (k < NH) srec[w] = (T)V.t1c[t1b_b + bp * NH + k];
+                    sval[w] = v;
+                }
             }
         }
         // per-row: a' stencil (off-diagonal part in registers; unused slots
@@ -481,7 +499,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
         const double* pval = P.pp_val + ch.pp_col_off;
         for (int bp = tid; bp < np2; bp += NT) {
             const int ab = ap * np2 + bp;
-            srec[bp * kLatNb + 7] = (pptr[ab + 1] > pptr[ab]) ? (T)pval[pptr[ab]] : T(0);
+            srec[bp * RW + RW - 1] = (pptr[ab + 1] > pptr[ab]) ? (T)pval[pptr[ab]] : T(0);
             sdp[bp] = (T)(da + V.dpc[ch.pb2 + bp]);
         }
         cp_async_wait_all();
@@ -526,6 +544,48 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
             // one element (b', i', j') given its terms along a
             auto element = [&](int bp, int eb, const T (&nb)[kLatNa], const T (&gv)[NH]) {
                 const T x = s_hp[eb];
+                if constexpr (PAIR) {
+                    float2 pr[8];
+                    int so[8];
+                    {
+                        const float* rp = reinterpret_cast<const float*>(srec) + bp * RW;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const float4 f = *reinterpret_cast<const float4*>(rp + 4 * u);
+                            pr[2 * u] = make_float2(f.x, f.y);
+                            pr[2 * u + 1] = make_float2(f.z, f.w);
+                        }
+                    }
+                    lds8(soff + bp * kLatNb, so);
+                    // (f_pp along b, rank-h part along b)
+                    float2 p1 = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < kLatNb - 1; ++q)
+                        p1 = __ffma2_rn(pr[q], make_float2(s_hp[so[q]], g_hp[q * NHP]), p1);
+                    // (X_hh along i, X_hh along j)
+                    float2 p2 = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int k = 0; k < NH; ++k)
+                        p2 = __ffma2_rn(x12[k], make_float2(s_col[eb + k * NH], s_row[eb + k]), p2);
+                    // (f_pp neighbours along a, rank-h part along a)
+                    float2 p3 = make_float2(adiag * x, 0.f);
+#pragma unroll
+                    for (int q = 0; q < kLatNa; ++q)
+                        p3 = __ffma2_rn(make_float2(aval[q], t1a[q]), make_float2(nb[q], gv[q]), p3);
+#pragma unroll
+                    for (int k = kLatNa; k < NH; ++k) p3.y = fmaf(t1a[k], gv[k], p3.y);
+                    const T t1bj = srec[bp * RW + 2 * jp + 1];
+                    const T lad = (hh + pr[7].y) * (x + t1ai * t1bj);
+                    const T acc = ((p3.x - p3.y) + (p1.x - p1.y)) + ((p2.x + p2.y) + lad);
+                    const T dd = -(sdp[bp] + dh);
+                    const T tn = x + lat_div(acc, dd);
+                    const T out = m * x + om * tn;
+                    __stcg(Bout + eb, out);
+                    const T d = out - x;
+                    if (Eout) __stcg(Eout + eb, d);
+                    nrm_row += d * d;
+                    return;
+                }
                 T rec[8], sv[8];
                 int so[8];
                 lds8(srec + bp * kLatNb, rec);
@@ -1026,7 +1086,7 @@ int64_t smem_limit() {
 // ladders, short f_pp rows) and its shared memory fits.
 bool use_lat(const nlb_struct_problem* P, size_t el) {
     return P->uniform_nh == 7 && P->diag_ladders && P->max_fpp_offdiag <= kLatNa &&
-           lat_smem(P->max_row, 7, (int64_t)el).total + 1024 <= smem_limit();
+           lat_smem(P->max_row, 7, (int64_t)el, el == 4).total + 1024 <= smem_limit();
 }
 
 int valid(const nlb_struct_problem* P, const nlb_struct_state* S) {
@@ -1042,10 +1102,10 @@ int valid(const nlb_struct_problem* P, const nlb_struct_state* S) {
 
 // The lattice T2 kernel with NT threads per block (NT / 49 hole-pair groups)
 // and at least MINB resident blocks per SM.
-template <typename T, int NT, int MINB>
+template <typename T, int NT, int MINB, bool PAIR = false>
 void launch_lat(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t st) {
-    const int64_t sm = lat_smem(P->max_row, 7, sizeof(T)).total;
-    auto kern = k_t2_lat<T, 7, NT, MINB>;
+    const int64_t sm = lat_smem(P->max_row, 7, sizeof(T), PAIR).total;
+    auto kern = k_t2_lat<T, 7, NT, MINB, PAIR>;
     const int bps = blocks_per_sm(reinterpret_cast<const void*>(kern), sm, NT);
     int64_t grid = (int64_t)num_sms() * bps;
     if (grid > P->n_rows) grid = P->n_rows;
@@ -1070,7 +1130,9 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
                 // bits 16-19), see nlb_struct_problem
                 if constexpr (sizeof(T) == 4) {
                     const int v = P->tune & 15;
-                    if (v == 1) launch_lat<T, 512, 1>(P, S, st);
+                    if (v == 3) launch_lat<T, 512, 1, true>(P, S, st);
+                    else if (v == 4) launch_lat<T, 384, 1, true>(P, S, st);
+                    else if (v == 1) launch_lat<T, 512, 1>(P, S, st);
                     else if (v == 2) launch_lat<T, 384, 1>(P, S, st);
                     else launch_lat<T, 256, 2>(P, S, st);
                 } else {

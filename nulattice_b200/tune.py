@@ -21,7 +21,7 @@ import torch
 from . import _lib
 from .ccsd import _mp2_t1, ctypes_void
 
-FWD_F32 = {0: "256x2", 1: "512x1", 2: "384x1"}
+FWD_F32 = {0: "256x2", 1: "512x1", 2: "384x1", 3: "512x1 x2", 4: "384x1 x2"}
 FWD_F64 = {0: "512x1", 1: "256x1"}
 LAM_F32 = {0: "256x2", 1: "512x1"}
 

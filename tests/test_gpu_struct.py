@@ -158,10 +158,24 @@ def _lattice_engine(L, A, general=False):
 def test_lattice_t2_kernel_matches_general_kernel(L, precision, tol):
     """Seven-hole lattice T2 kernel vs the general row kernel: same steps,
     DIIS pulses included, on rows of 20, 63 and 118 particles per label."""
+    _lattice_vs_general(L, precision, tol, 0)
+
+
+@pytest.mark.parametrize("L", [3, 4, 5, 6])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4])
+def test_fp32_lattice_launch_shapes_match_general_kernel(L, shape):
+    """Every other FP32 launch shape of the lattice T2 update (512 and 384
+    threads, scalar and packed FP32x2 sums) against the general row kernel,
+    up to rows of 209 particles per label."""
+    _lattice_vs_general(L, "mixed", 1e-5, shape)
+
+
+def _lattice_vs_general(L, precision, tol, shape):
     from nulattice_b200.ccsd import solve_structured
     out = []
     for general in (False, True):
         eng = _lattice_engine(L, 28, general)
+        eng.prob.tune = shape
         info = {}
         e, t1, t2 = solve_structured(eng, eps=0.0, maxSteps=11, max_diis=4, precision=precision,
                                      mixed_eps=0.0, refine=False, t2_format="compact", info=info)
