@@ -60,19 +60,67 @@ constexpr int kRowThreads = 256;   // T2 row kernel
 // gives the rank-h part of X_pp t2 along a, and it holds the T1 Fock term
 // f_ck t2_acik for particles of label g2.
 // The dressed-Fock tables (from t1) and Ga (from t2) in one launch: they
-// read different amplitudes and are independent.
+// read different amplitudes and are independent.  The first n_channels *
+// max_nh * gx blocks each take one chunk of a Ga row (channel, hole k'),
+// read its f_ph column list once and stream the chunk coalesced, four
+// elements per thread; the blocks after them form the dressed-Fock tables.
+constexpr int kGaVec = 4;    // Ga elements per thread
+
 template <typename T>
-__global__ void k_prep_ga(nlb_struct_problem P, nlb_struct_state S, int64_t nprep) {
+__global__ void __launch_bounds__(kThreads) k_prep_ga(nlb_struct_problem P, nlb_struct_state S, int64_t nprep,
+                                                      int gx) {
     const nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
-    const double* t1 = S.t1[c->parity];
-    const T* B = static_cast<const T*>(S.t2[c->parity]);
-    T* G = static_cast<T*>(S.g);
-    const int64_t ng = (c->ccs || P.n_t2 == 0) ? 0 : P.n_g;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nprep + ng; u += stride) {
-        if (u < nprep) prep_body(P, t1, S.prep, u);
-        else G[u - nprep] = ga_element(P, B, u - nprep);
+    const int64_t nga_blocks = (c->ccs || P.n_t2 == 0) ? 0 : (int64_t)P.n_channels * P.max_nh * gx;
+    const int64_t all_ga = (int64_t)P.n_channels * P.max_nh * gx;
+    if ((int64_t)blockIdx.x >= all_ga) {
+        const double* t1 = S.t1[c->parity];
+        const int64_t nb = gridDim.x - all_ga;
+        for (int64_t u = ((int64_t)blockIdx.x - all_ga) * blockDim.x + threadIdx.x; u < nprep; u += nb * blockDim.x)
+            prep_body(P, t1, S.prep, u);
+        return;
+    }
+    if ((int64_t)blockIdx.x >= nga_blocks) return;
+    const int yr = blockIdx.x / gx, bx = blockIdx.x - yr * gx;
+    const int ci = yr / P.max_nh, kq = yr - ci * P.max_nh;
+    const nlb_channel& ch = P.chan[ci];
+    if (kq >= ch.nh1) return;
+    const int rowlen = ch.np2 * ch.nh1 * ch.nh2;
+    const int row = ch.hb1 + kq;
+    const int q0 = P.fph_ptr[row], q1 = P.fph_ptr[row + 1];
+    const T* __restrict__ Bc = static_cast<const T*>(S.t2[c->parity]) + ch.offset;
+    T* __restrict__ Gr = static_cast<T*>(S.g) + ch.ga_off + (int64_t)kq * rowlen;
+    // Ga[k'][e] = sum_c f_ck B[c'][e], the f_ph entries of hole k in order
+    constexpr int QR = 8;    // entries kept in registers (a lattice hole has at most six)
+    T fv[QR];
+    int64_t fo[QR];
+#pragma unroll
+    for (int u = 0; u < QR; ++u) {
+        fv[u] = (q0 + u < q1) ? (T)P.fph_val[q0 + u] : T(0);
+        fo[u] = (q0 + u < q1) ? (int64_t)P.fph_col[q0 + u] * rowlen : 0;
+    }
+    const int nq = q1 - q0;
+    const int step = gx * blockDim.x * kGaVec;
+    for (int e0 = bx * blockDim.x * kGaVec + threadIdx.x; e0 < rowlen; e0 += step) {
+        T v[kGaVec];
+#pragma unroll
+        for (int r = 0; r < kGaVec; ++r) {
+            const int e = e0 + r * (int)blockDim.x;
+            T acc = T(0);
+            if (e < rowlen) {
+#pragma unroll
+                for (int u = 0; u < QR; ++u)
+                    if (u < nq) acc += fv[u] * Bc[fo[u] + e];
+                for (int q = q0 + QR; q < q1; ++q)
+                    acc += (T)P.fph_val[q] * Bc[(int64_t)P.fph_col[q] * rowlen + e];
+            }
+            v[r] = acc;
+        }
+#pragma unroll
+        for (int r = 0; r < kGaVec; ++r) {
+            const int e = e0 + r * (int)blockDim.x;
+            if (e < rowlen) Gr[e] = v[r];
+        }
     }
 }
 
@@ -662,11 +710,11 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
 // energy sum_ai f_ai t1'_ai (coupled_cluster.py:342-414, 265-286).
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nlb_struct_state S) {
-    // One warp per amplitude t1[a, i] of matching labels (the others are
-    // zero for label-conserving inputs and stay zero); the lanes share the
-    // terms of its residual: the T2 Fock terms of the channels holding the
-    // label (F2, or the Ga diagonal), the f_pp neighbours of a and the hole
-    // mixing over the label's holes.
+    // Sixteen lanes per amplitude t1[a, i] of matching labels (the others
+    // are zero for label-conserving inputs and stay zero); the lanes share
+    // the terms of its residual: the T2 Fock terms of the channels holding
+    // the label (F2, or the Ga diagonal), the f_pp neighbours of a and the
+    // hole mixing over the label's holes.
     nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
     const int par = c->parity;
@@ -689,9 +737,15 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
             if (E1) E1[idx] = 0.0;
         }
     }
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarps = stride >> 5;
-    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < P.n_t1c; q += nwarps) {
+    // sixteen lanes per amplitude (two amplitudes per warp): every term of
+    // its residual is an independent load, so one wave covers all of them
+    const int lane = threadIdx.x & 15;
+    const int64_t nhalf = stride >> 4;
+    for (int64_t q0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+         q0 - (((int64_t)threadIdx.x >> 4) & 1) < P.n_t1c; q0 += nhalf) {
+        // both halves of a warp stay in the loop until neither has work
+        const bool live = q0 < P.n_t1c;
+        const int64_t q = live ? q0 : P.n_t1c - 1;
         const int g = find_label(P.t1c_base, P.n_labels, q);
         const int nh = P.h_base[g + 1] - P.h_base[g];
         const int loc = (int)(q - P.t1c_base[g]);
@@ -701,27 +755,48 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
         const int64_t idx = (int64_t)a * h + i;
         double part = 0.0;
         if (!c->ccs) {
-            for (int cc = 0; cc < P.n_channels; ++cc) {
-                const nlb_channel& ch = P.chan[cc];
-                if (ch.g1 == g) {
-                    if (lane == 0) part += (double)F2[ch.f2_off + (int64_t)ap * ch.nh1 + ip];
-                } else if (ch.g2 == g && lane < ch.nh1) {
-                    const int nhp = ch.nh1 * ch.nh2;
-                    const int64_t rowlen = (int64_t)ch.np2 * nhp;
-                    part += (double)Ga[ch.ga_off + (int64_t)ap * nhp + ip + lane * rowlen + lane * ch.nh2];
+            // channels in groups of four whose loads go out together (the
+            // sum keeps the channel order)
+            for (int c0 = 0; c0 < P.n_channels; c0 += 4) {
+                double cp[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    cp[u] = 0.0;
+                    if (c0 + u >= P.n_channels) continue;
+                    const nlb_channel& ch = P.chan[c0 + u];
+                    if (ch.g1 == g) {
+                        if (lane == 0) cp[u] = (double)F2[ch.f2_off + (int64_t)ap * ch.nh1 + ip];
+                    } else if (ch.g2 == g && lane < ch.nh1) {
+                        const int nhp = ch.nh1 * ch.nh2;
+                        const int64_t rowlen = (int64_t)ch.np2 * nhp;
+                        cp[u] = (double)Ga[ch.ga_off + (int64_t)ap * nhp + ip + lane * rowlen + lane * ch.nh2];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) part += cp[u];
+                // holes of a channel beyond the sixteen lanes
+                for (int u = 0; u < 4 && c0 + u < P.n_channels; ++u) {
+                    const nlb_channel& ch = P.chan[c0 + u];
+                    if (ch.g1 != g && ch.g2 == g && ch.nh1 > 16) {
+                        const int nhp = ch.nh1 * ch.nh2;
+                        const int64_t rowlen = (int64_t)ch.np2 * nhp;
+                        for (int k = lane + 16; k < ch.nh1; k += 16)
+                            part += (double)Ga[ch.ga_off + (int64_t)ap * nhp + ip + k * rowlen + k * ch.nh2];
+                    }
                 }
             }
         }
         const int r = pb + ap;
-        const int q0 = P.fpp_ptr[r], q1 = P.fpp_ptr[r + 1];
-        for (int qq = q0 + lane; qq < q1; qq += 32)
+        const int f0 = P.fpp_ptr[r], f1 = P.fpp_ptr[r + 1];
+        for (int qq = f0 + lane; qq < f1; qq += 16)
             part += P.fpp_val[qq] * t1[(int64_t)P.p_ord[pb + P.fpp_col[qq]] * h + i];
-        if (lane < nh) {
-            const int k = P.h_ord[P.h_base[g] + lane];
+        for (int kk = lane; kk < nh; kk += 16) {
+            const int k = P.h_ord[P.h_base[g] + kk];
             part += t1[(int64_t)a * h + k] * (V.Xh1[(int64_t)k * h + i] - 0.5 * V.Q[(int64_t)k * h + i]);
         }
-        part = warp_sum(part);
-        if (lane == 0) {
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0 && live) {
             const double H1 = P.f_ph[idx] + part;
             const double D1 = -(V.dXp1[a] + V.Xh1[(int64_t)i * h + i]);
             const double x = t1[idx];
@@ -1118,8 +1193,12 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
         case NLB_STAGE_PREP: {
             const int64_t nprep = (int64_t)P->h * P->h + 2 * (int64_t)P->p + P->n_t1c + P->n_xc + P->h;
             // the dressed-Fock tables and Ga in one launch (the GTERMS stage is then empty)
-            const int64_t ng = P->n_t2 > 0 ? P->n_g : 0;
-            k_prep_ga<T><<<grid_for(k_prep_ga<T>, nprep + ng), kThreads, 0, st>>>(*P, *S, nprep);
+            const int64_t per_blk = (int64_t)kThreads * kGaVec;
+            const int64_t gx = P->n_t2 > 0 ? (P->max_row + per_blk - 1) / per_blk : 1;
+            const int64_t ga_blocks = (int64_t)P->n_channels * P->max_nh * gx;
+            int64_t gp = (nprep + kThreads - 1) / kThreads;
+            if (gp < 1) gp = 1;
+            k_prep_ga<T><<<(unsigned)(ga_blocks + gp), kThreads, 0, st>>>(*P, *S, nprep, (int)gx);
             break;
         }
         case NLB_STAGE_GTERMS:
@@ -1150,7 +1229,7 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
             }
             break;
         case NLB_STAGE_T1:
-            k_t1_update<T><<<grid_for(k_t1_update<T>, 32 * (int64_t)P->n_t1c), kThreads, 0, st>>>(*P, *S);
+            k_t1_update<T><<<grid_for(k_t1_update<T>, 16 * (int64_t)P->n_t1c), kThreads, 0, st>>>(*P, *S);
             break;
         default:
             k_finish<<<1, 32, 0, st>>>(S->ctrl);

@@ -73,15 +73,38 @@ __device__ __forceinline__ double q_entry(const nlb_struct_problem& P, const dou
     const int g = P.h_label[k];
     const int row = P.h_base[g] + P.h_loc[k];
     const int pb = P.p_base[g];
+    // entries in batches of eight whose loads go out together (a lattice
+    // hole has at most six particle neighbours); the sum keeps their order
     double q = 0.0;
-    for (int e = P.fph_ptr[row]; e < P.fph_ptr[row + 1]; ++e)
-        q += P.fph_val[e] * t1[(int64_t)P.p_ord[pb + P.fph_col[e]] * P.h + i];
+    const int e0 = P.fph_ptr[row], e1 = P.fph_ptr[row + 1];
+    for (int b = e0; b < e1; b += 8) {
+        double tv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            tv[u] = (b + u < e1) ? t1[(int64_t)P.p_ord[pb + P.fph_col[b + u]] * P.h + i] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (b + u < e1) q += P.fph_val[b + u] * tv[u];
+    }
     return q;
 }
 
 __device__ __forceinline__ double s_entry(const nlb_struct_problem& P, const double* t1, int a) {
+    // loads in batches of eight that go out together; the sum keeps the order
+    const double* f = P.f_ph + (int64_t)a * P.h;
+    const double* t = t1 + (int64_t)a * P.h;
     double s = 0.0;
-    for (int k = 0; k < P.h; ++k) s += P.f_ph[(int64_t)a * P.h + k] * t1[(int64_t)a * P.h + k];
+    for (int k = 0; k < P.h; k += 8) {
+        double fv[8], tv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            fv[u] = (k + u < P.h) ? f[k + u] : 0.0;
+            tv[u] = (k + u < P.h) ? t[k + u] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (k + u < P.h) s += fv[u] * tv[u];
+    }
     return s;
 }
 
