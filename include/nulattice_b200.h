@@ -88,6 +88,14 @@ typedef struct {
     const double *f_hh;           /* [h*h] dense */
     const int32_t *hh_ptr, *hh_col; const double *hh_val;     /* hole-hole ladder CSR */
     const int32_t *pp_ptr, *pp_col; const double *pp_val;     /* particle-particle ladder CSR */
+    /* Optional index tables that shorten the chains of dependent loads in
+       the step kernels; NULL: the same indices are derived from the tables
+       above. */
+    const int32_t *h_row;         /* [h] label-ordered f_ph row of hole k: h_base[h_label[k]] + h_loc[k] */
+    const int32_t *fph_prow;      /* [nnz f_ph] particle index of each f_ph entry: p_ord[p_base[g] + fph_col] */
+    const int32_t *fpp_prow;      /* [nnz f_pp] particle index of each f_pp entry: p_ord[p_base[g] + fpp_col] */
+    const int32_t *t1c_idx;       /* [n_t1c] flat t1 index a * h + i of each t1c entry */
+    const int32_t *xc_ki;         /* [n_xc] k * h + i (global holes) of each X_hh entry */
 } nlb_struct_problem;
 
 /* Device-resident solver state shared by the kernels of one solve. */

@@ -40,7 +40,8 @@ class StructProblem(ctypes.Structure):
                                 "p_ord", "h_ord", "p_label", "h_label",
                                 "p_loc", "h_loc", "p_base", "h_base", "fpp_ptr", "fpp_col", "fpp_val",
                                 "fpp_diag", "fph_ptr", "fph_col", "fph_val", "f_ph", "f_hh",
-                                "hh_ptr", "hh_col", "hh_val", "pp_ptr", "pp_col", "pp_val")]
+                                "hh_ptr", "hh_col", "hh_val", "pp_ptr", "pp_col", "pp_val",
+                                "h_row", "fph_prow", "fpp_prow", "t1c_idx", "xc_ki")]
 
 
 class Ctrl(ctypes.Structure):

@@ -141,6 +141,23 @@ class StructuredEngine:
         T["hh_val"] = f64(cat(hh_val, np.float64))
         T["pp_ptr"] = i32(cat(pp_ptr, np.int32)); T["pp_col"] = i32(cat(pp_col, np.int32))
         T["pp_val"] = f64(cat(pp_val, np.float64))
+        # index tables that spare the step kernels chains of dependent loads
+        h_lab = np.asarray(pl.h_label, np.int64)
+        T["h_row"] = i32(np.asarray(pl.h_base, np.int64)[h_lab] + np.asarray(pl.h_loc, np.int64))
+        fph_rows = np.repeat(np.arange(len(pl.fph_ptr) - 1), np.diff(pl.fph_ptr))
+        fph_lab = np.searchsorted(np.asarray(pl.h_base, np.int64), fph_rows, side="right") - 1
+        fpp_rows = np.repeat(np.arange(len(pl.fpp_ptr) - 1), np.diff(pl.fpp_ptr))
+        fpp_lab = np.searchsorted(np.asarray(pl.p_base, np.int64), fpp_rows, side="right") - 1
+        pb = np.asarray(pl.p_base, np.int64)
+        T["fph_prow"] = i32(p_ord[pb[fph_lab] + np.asarray(pl.fph_col, np.int64)] if len(fph_rows) else [0])
+        T["fpp_prow"] = i32(p_ord[pb[fpp_lab] + np.asarray(pl.fpp_col, np.int64)] if len(fpp_rows) else [0])
+        t1c_idx, xc_ki = [], []
+        for g in range(G):
+            P_, H_ = np.asarray(pl.p_of[g], np.int64), np.asarray(pl.h_of[g], np.int64)
+            t1c_idx.append((P_[:, None] * pl.h + H_[None, :]).ravel())
+            xc_ki.append((H_[:, None] * pl.h + H_[None, :]).ravel())
+        T["t1c_idx"] = i32(cat(t1c_idx, np.int64))
+        T["xc_ki"] = i32(cat(xc_ki, np.int64))
         self.tables = T
         prob = _lib.StructProblem()
         prob.p, prob.h, prob.n_labels, prob.n_channels = pl.p, pl.h, G, len(pl.channels)

@@ -746,12 +746,25 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
         // both halves of a warp stay in the loop until neither has work
         const bool live = q0 < P.n_t1c;
         const int64_t q = live ? q0 : P.n_t1c - 1;
-        const int g = find_label(P.t1c_base, P.n_labels, q);
+        int g, a, i, ap, ip;
+        if (P.t1c_idx) {
+            const int id = P.t1c_idx[q];
+            a = id / h;
+            i = id - a * h;
+            g = P.p_label[a];
+            ap = P.p_loc[a];
+            ip = P.h_loc[i];
+        } else {
+            g = find_label(P.t1c_base, P.n_labels, q);
+            const int nh_ = P.h_base[g + 1] - P.h_base[g];
+            const int loc = (int)(q - P.t1c_base[g]);
+            ap = loc / nh_;
+            ip = loc - ap * nh_;
+            a = P.p_ord[P.p_base[g] + ap];
+            i = P.h_ord[P.h_base[g] + ip];
+        }
         const int nh = P.h_base[g + 1] - P.h_base[g];
-        const int loc = (int)(q - P.t1c_base[g]);
-        const int ap = loc / nh, ip = loc - ap * nh;
         const int pb = P.p_base[g];
-        const int a = P.p_ord[pb + ap], i = P.h_ord[P.h_base[g] + ip];
         const int64_t idx = (int64_t)a * h + i;
         double part = 0.0;
         if (!c->ccs) {
@@ -788,8 +801,10 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
         }
         const int r = pb + ap;
         const int f0 = P.fpp_ptr[r], f1 = P.fpp_ptr[r + 1];
-        for (int qq = f0 + lane; qq < f1; qq += 16)
-            part += P.fpp_val[qq] * t1[(int64_t)P.p_ord[pb + P.fpp_col[qq]] * h + i];
+        for (int qq = f0 + lane; qq < f1; qq += 16) {
+            const int c2 = P.fpp_prow ? P.fpp_prow[qq] : P.p_ord[pb + P.fpp_col[qq]];
+            part += P.fpp_val[qq] * t1[(int64_t)c2 * h + i];
+        }
         for (int kk = lane; kk < nh; kk += 16) {
             const int k = P.h_ord[P.h_base[g] + kk];
             part += t1[(int64_t)a * h + k] * (V.Xh1[(int64_t)k * h + i] - 0.5 * V.Q[(int64_t)k * h + i]);
@@ -851,6 +866,7 @@ __global__ void k_finish(nlb_ctrl* c) {
     c->dt1_sq = 0.0;
     c->dt2_sq = 0.0;
 }
+
 
 // ---------------------------------------------------------------- DIIS ----
 // Gram matrix of the stored error vectors: <e_a, e_b> over the dense t1 and

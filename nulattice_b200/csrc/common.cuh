@@ -70,12 +70,25 @@ __device__ __forceinline__ int find_label(const int32_t* base, int G, int64_t u)
 
 // Q[k,i] = sum_c f_ck t1_ci using the f_ph column list of hole k.
 __device__ __forceinline__ double q_entry(const nlb_struct_problem& P, const double* t1, int k, int i) {
-    const int g = P.h_label[k];
-    const int row = P.h_base[g] + P.h_loc[k];
-    const int pb = P.p_base[g];
     // entries in batches of eight whose loads go out together (a lattice
     // hole has at most six particle neighbours); the sum keeps their order
     double q = 0.0;
+    if (P.h_row && P.fph_prow) {
+        const int row = P.h_row[k];
+        const int e0 = P.fph_ptr[row], e1 = P.fph_ptr[row + 1];
+        for (int b = e0; b < e1; b += 8) {
+            double tv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) tv[u] = (b + u < e1) ? t1[(int64_t)P.fph_prow[b + u] * P.h + i] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (b + u < e1) q += P.fph_val[b + u] * tv[u];
+        }
+        return q;
+    }
+    const int g = P.h_label[k];
+    const int row = P.h_base[g] + P.h_loc[k];
+    const int pb = P.p_base[g];
     const int e0 = P.fph_ptr[row], e1 = P.fph_ptr[row + 1];
     for (int b = e0; b < e1; b += 8) {
         double tv[8];
@@ -130,6 +143,10 @@ __device__ void prep_body(const nlb_struct_problem& P, const double* t1, double*
     }
     u -= p;
     if (u < P.n_t1c) {
+        if (P.t1c_idx) {
+            V.t1c[u] = t1[P.t1c_idx[u]];
+            return;
+        }
         const int g = find_label(P.t1c_base, G, u);
         const int nh = P.h_base[g + 1] - P.h_base[g];
         const int loc = (int)(u - P.t1c_base[g]);
@@ -139,6 +156,12 @@ __device__ void prep_body(const nlb_struct_problem& P, const double* t1, double*
     }
     u -= P.n_t1c;
     if (u < P.n_xc) {
+        if (P.xc_ki) {
+            const int ki = P.xc_ki[u];
+            const int k = ki / h, i = ki - k * h;
+            V.xc[u] = -P.f_hh[ki] - q_entry(P, t1, k, i);
+            return;
+        }
         const int g = find_label(P.xc_base, G, u);
         const int nh = P.h_base[g + 1] - P.h_base[g];
         const int loc = (int)(u - P.xc_base[g]);

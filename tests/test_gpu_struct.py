@@ -185,3 +185,24 @@ def _lattice_vs_general(L, precision, tol, shape):
     assert ea == pytest.approx(eb, rel=tol)
     np.testing.assert_allclose(t1a, t1b, atol=tol * np.abs(t1b).max())
     np.testing.assert_allclose(t2a, t2b, atol=tol * np.abs(t2b).max())
+
+
+def test_index_tables_are_optional():
+    """The step kernels' index tables (hole rows, particle of each f_ph /
+    f_pp entry, flat t1 index, X_hh hole pair) only shorten load chains:
+    without them the same steps come out."""
+    from nulattice_b200.ccsd import solve_structured
+    out = []
+    for tables in (True, False):
+        eng = _lattice_engine(4, 28)
+        if not tables:
+            for name in ("h_row", "fph_prow", "fpp_prow", "t1c_idx", "xc_ki"):
+                setattr(eng.prob, name, None)
+        e, t1, t2 = solve_structured(eng, eps=0.0, maxSteps=10, max_diis=4, t2_format="compact")
+        out.append((e, t1.cpu().numpy(), t2.cpu().numpy()))
+    (ea, t1a, t2a), (eb, t1b, t2b) = out
+    # the two index paths may contract different products into FMAs: a few
+    # ulp per step, amplified by the ten steps and the DIIS pulse
+    assert ea == pytest.approx(eb, rel=1e-12)
+    np.testing.assert_allclose(t1a, t1b, rtol=0, atol=1e-10 * np.abs(t1b).max())
+    np.testing.assert_allclose(t2a, t2b, rtol=0, atol=1e-10 * np.abs(t2b).max())

@@ -121,7 +121,7 @@ def test_library_exports_declared_symbols():
         assert hasattr(L, s), s
     assert L.nlb_version() >= 1
     assert ctypes.sizeof(_lib.Ctrl) == 1064
-    assert ctypes.sizeof(_lib.StructProblem) == 320
+    assert ctypes.sizeof(_lib.StructProblem) == 360
 
 
 def test_lambda_and_batch_struct_layouts():
