@@ -318,9 +318,7 @@ def main():
     tfile = os.path.join(ROOT, "profiles", "t2_update_traffic.json")
     if os.path.exists(tfile):
         traffic = json.load(open(tfile)).get("bytes_per_launch")
-    shape = T.describe(int(eng.prob.tune))["t2_fp32"] or "256x2"
-    nt_, mb_ = shape.split("x")
-    roofline = {"kernel": f"k_t2_lat<float, 7, {nt_}, {mb_}>", "bound": "hbm", "achieved": achieved, "peak": peak,
+    roofline = {"kernel": T.t2_kernel_fp32(int(eng.prob.tune)), "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_us": k_ms * 1e3, "launches": len(m_k)}
 
@@ -418,7 +416,8 @@ def batch_leg(dev, peak_gbs, rank=0, ws=1):
             torch.cuda.synchronize(dev)
             t1 = time.perf_counter()
             info = {}
-            e, t1v, t2c = solve_structured(x.eng, eps=1e-10, maxSteps=500, t2_format="compact", info=info, **kw)
+            e, t1v, t2c = solve_structured(x.eng, eps=1e-10, maxSteps=500, t2_format="compact", info=info,
+                                           loop="eager", **kw)
             g = None
             if info["status"] == "converged":
                 try:
@@ -463,8 +462,9 @@ def batch_leg(dev, peak_gbs, rank=0, ws=1):
             "algorithm": "forward FP32 pulsed DIIS to 1e-8 + FP64 to 1e-10; Lambda FP32 DIIS to 1e-6 + FP64 to 1e-8 "
                          "(lattice), FP64 DIIS to 1e-8 (one hole per label); max 500 steps per phase",
             "sequential_fp64": "forward FP64 Jacobi + mixing to 1e-10, Lambda FP64 Jacobi to 1e-8, one instance at a time",
-            "sequential_note": "one-at-a-time times are wall clock per instance and include each engine's first "
-                               "graph captures, as a user solving instances one by one sees them"}
+            "sequential_note": "one-at-a-time times are wall clock per instance: forward launched from the host "
+                               "chunk by chunk (no graph build for a one-off solve), Lambda with its chunk graphs, "
+                               "as a user solving instances one by one sees them"}
 
 
 def adjoint_leg(dev):

@@ -35,6 +35,13 @@ def describe(w):
             "lambda_chunks": (w >> 8) & 255 or "auto", "t2_fp64": FWD_F64.get((w >> 16) & 15)}
 
 
+def t2_kernel_fp32(w):
+    """Template name of the FP32 lattice T2 kernel the word selects."""
+    v = w & 15
+    nt, mb = {0: (256, 2), 1: (512, 1), 2: (384, 1), 3: (512, 1), 4: (384, 1)}.get(v, (256, 2))
+    return f"k_t2_lat<float, 7, {nt}, {mb}, {'true' if v in (3, 4) else 'false'}>"
+
+
 def _cache_path():
     return os.environ.get("NLB_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "nulattice_b200",
                                                          "tune.json"))
