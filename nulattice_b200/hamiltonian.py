@@ -233,6 +233,43 @@ def _three_body_no2b(rows, is_hole, loc, p, h):
     return de, df_pp, df_hh, conv
 
 
+def _canonical_block(shape, idx, val, add=None):
+    """The non-zero entries, in lexicographic index order, of the dense block
+    that ``_dense_assign(shape, idx, val)`` followed by ``np.add.at`` of the
+    entries ``add = (idx, val)`` would hold: the last write of a repeated
+    two-body key wins, the added entries are summed after it in their order,
+    and zeros are dropped.  Built without the dense block (4.4 GB for v_pphh
+    at L=6, A=28)."""
+    shape = tuple(int(x) for x in shape)
+    idx = np.asarray(idx, np.int64).reshape(-1, len(shape))
+    val = np.asarray(val, np.float64).reshape(-1)
+    key = np.ravel_multi_index(tuple(idx.T), shape) if len(val) else np.zeros(0, np.int64)
+    uk, first = np.unique(key[::-1], return_index=True)
+    v = val[len(key) - 1 - first] if len(val) else np.zeros(0)
+    if add is not None and len(add[1]):
+        ak = np.ravel_multi_index(tuple(np.asarray(add[0], np.int64).T), shape)
+        allk = np.concatenate([uk, ak])
+        allv = np.concatenate([v, np.asarray(add[1], np.float64)])
+        order = np.argsort(allk, kind="stable")   # the two-body value first, then the sums in order
+        ks, vs = allk[order], allv[order]
+        first_of = np.concatenate(([True], ks[1:] != ks[:-1]))
+        seg = np.cumsum(first_of) - 1
+        v = np.zeros(int(first_of.sum()))
+        np.add.at(v, seg, vs)                       # in order, as the dense path's np.add.at
+        uk = ks[first_of]
+    keep = v != 0
+    return np.stack(np.unravel_index(uk[keep], shape), 1).astype(np.int64), v[keep]
+
+
+def _trace_13(shape, idx, val, out_shape):
+    """sum_i X[a, i, b, i] of a COO block (``einsum("aibi->ab")``)."""
+    out = np.zeros(out_shape)
+    m = idx[:, 1] == idx[:, 3]
+    if m.any():
+        np.add.at(out, (idx[m, 0], idx[m, 2]), val[m])
+    return out
+
+
 def normal_ordered_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, kinetic=1.0):
     """``get_norm_ordered_ham`` for the lattice contact Hamiltonian
     (``CCM/coupled_cluster.py:752-832`` with ``sparse=True, NO2B=True``).
@@ -254,6 +291,8 @@ def normal_ordered_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, kinetic=1
 
     b = _sort_two_body(contact_rows(vT1, vS1, L), is_hole, loc)
     shapes = {"pphh": (p, p, h, h), "phph": (p, h, p, h), "phhh": (p, h, h, h), "hhhh": (h, h, h, h)}
+    if not dense:
+        return _normal_ordered_sparse(L, b, shapes, hole, part, is_hole, loc, p, h, w3, kinetic)
     dense2 = {k: _dense_assign(shapes[k], *b[k]) for k in shapes}
 
     # Fock matrices: kinetic entry plus the hole trace of the two-body blocks,
@@ -285,13 +324,47 @@ def normal_ordered_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, kinetic=1
                                                       nb["pppp"][1][:, None]], 1)])
     # reference energy (CCM/coupled_cluster.py:288-317)
     e_ref = float(np.trace(f_hh) - 0.5 * np.einsum("ijij->", dense2["hhhh"]) + e3)
-    if dense:
-        blocks = [dense2[k] for k in ("pphh", "phph", "phhh", "hhhh")]
-    else:
-        blocks = []
-        for k in ("pphh", "phph", "phhh", "hhhh"):
-            idx = np.argwhere(dense2[k] != 0)
-            blocks.append(Block(shapes[k], idx, dense2[k][tuple(idx.T)]))
+    blocks = [dense2[k] for k in ("pphh", "phph", "phhh", "hhhh")]
+    return e_ref, [f_pp, f_ph, f_hh], [sparse_rows["pppp"], sparse_rows["ppph"]] + blocks
+
+
+def _normal_ordered_sparse(L, b, shapes, hole, part, is_hole, loc, p, h, w3, kinetic):
+    """``normal_ordered_hamiltonian(..., dense=False)``: the same numbers with
+    the four two-body blocks kept as COO :class:`Block` objects from the
+    start (entries and their order as the dense path's non-zeros)."""
+    n = 4 * L ** 3
+    e3, nb = 0.0, {}
+    dfpp = dfhh = None
+    if w3 != 0.0:
+        e3, dfpp, dfhh, nb = _three_body_no2b(three_body_rows(w3, L), is_hole, loc, p, h)
+    # the Fock traces see the two-body entries only; the three-body ones are
+    # added to the blocks afterwards (as in the dense path)
+    two = {k: _canonical_block(shapes[k], *b[k]) for k in shapes}
+    coo = {k: (_canonical_block(shapes[k], *b[k], add=nb[k]) if k in nb else two[k]) for k in shapes}
+    T = np.zeros((n, n)); has_t = np.zeros((n, n), bool)
+    kr = kinetic_rows(L)
+    ti, tj = kr[:, 0].astype(np.int64), kr[:, 1].astype(np.int64)
+    np.add.at(T, (ti, tj), float(kinetic) * kr[:, 2])
+    has_t[ti, tj] = True
+    f_pp = T[np.ix_(part, part)] + _trace_13(shapes["phph"], *two["phph"], (p, p))
+    f_ph = T[np.ix_(part, hole)] + _trace_13(shapes["phhh"], *two["phhh"], (p, h))
+    f_hh = T[np.ix_(hole, hole)] + _trace_13(shapes["hhhh"], *two["hhhh"], (h, h))
+    f_pp = np.where(has_t[np.ix_(part, part)], f_pp, 0.0)
+    f_ph = np.where(has_t[np.ix_(part, hole)], f_ph, 0.0)
+    f_hh = np.where(has_t[np.ix_(hole, hole)], f_hh, 0.0)
+    sparse_rows = {k: np.concatenate([b[k][0].astype(np.float64), b[k][1][:, None]], 1)
+                   for k in ("pppp", "ppph")}
+    if w3 != 0.0:
+        f_pp = f_pp + dfpp
+        f_hh = f_hh + dfhh
+        if len(nb["pppp"][1]):
+            sparse_rows["pppp"] = np.concatenate(
+                [sparse_rows["pppp"], np.concatenate([nb["pppp"][0].astype(np.float64),
+                                                      nb["pppp"][1][:, None]], 1)])
+    hi, hv = coo["hhhh"]
+    diag = (hi[:, 0] == hi[:, 2]) & (hi[:, 1] == hi[:, 3])
+    e_ref = float(np.trace(f_hh) - 0.5 * np.sum(hv[diag]) + e3)
+    blocks = [Block(shapes[k], *coo[k]) for k in ("pphh", "phph", "phhh", "hhhh")]
     return e_ref, [f_pp, f_ph, f_hh], [sparse_rows["pppp"], sparse_rows["ppph"]] + blocks
 
 

@@ -34,12 +34,23 @@ def test_builder_matches_reference(tag):
     assert _canon(two[1]) == pytest.approx(_canon(tr[1]))
 
 
-def test_builder_sparse_blocks_equal_dense():
-    e1, f1, t1 = ham.normal_ordered_hamiltonian(3, ham.closed_shell_holes(3, 4), -6, -6, 2, dense=True)
-    e2, f2, t2 = ham.normal_ordered_hamiltonian(3, ham.closed_shell_holes(3, 4), -6, -6, 2, dense=False)
+@pytest.mark.parametrize("L,A,v,w,kin", [(3, 4, -6, 2, 1.0), (4, 4, -3.3, 0.7, 1.0), (4, 28, -6, 2, 1.0),
+                                         (3, 28, 1, 1, 0.0), (5, 28, -4.1, 1.3, 1.0)])
+def test_builder_sparse_blocks_equal_dense(L, A, v, w, kin):
+    """The sparse builder (no dense block is ever formed) gives bit for bit
+    the dense builder's numbers, which the reference goldens pin."""
+    e1, f1, t1 = ham.normal_ordered_hamiltonian(L, ham.closed_shell_holes(L, A), v, v, w, dense=True, kinetic=kin)
+    e2, f2, t2 = ham.normal_ordered_hamiltonian(L, ham.closed_shell_holes(L, A), v, v, w, dense=False, kinetic=kin)
     assert e1 == e2
+    for a, b in zip(f1, f2):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(t1[:2], t2[:2]):
+        np.testing.assert_array_equal(a, b)
     for a, b in zip(t1[2:], t2[2:]):
         np.testing.assert_array_equal(a, b.to_dense())
+        assert np.all(b.values != 0)
+        key = np.ravel_multi_index(tuple(b.indices.T), b.shape)
+        assert np.all(np.diff(key) > 0)   # unique, in the dense non-zeros' order
 
 
 def test_units_and_holes():
