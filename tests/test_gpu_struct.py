@@ -206,3 +206,19 @@ def test_index_tables_are_optional():
     assert ea == pytest.approx(eb, rel=1e-12)
     np.testing.assert_allclose(t1a, t1b, rtol=0, atol=1e-10 * np.abs(t1b).max())
     np.testing.assert_allclose(t2a, t2b, rtol=0, atol=1e-10 * np.abs(t2b).max())
+
+
+@pytest.mark.parametrize("key", [(2, -3.0, 1.0), (3, -3.0, 1.0)])
+def test_plane_wave_inputs_match_reference(key):
+    """Plane-wave inputs (diagonal one-body part, non-zero v_pphh / v_phph /
+    v_phhh) go to the general engine and give the reference's correlation
+    energy."""
+    from nulattice_b200 import planewave as PW
+    from test_planewave import REF
+    L, v, w = key
+    e_ref, fock, two = PW.plane_wave_hamiltonian(L, PW.momentum_holes(L, 4), v, v, w, dense=False)
+    info = {}
+    e, t1, t2 = ccsd_solver(fock, two, eps=1e-13, maxSteps=3000, max_diis=10, device=DEV, info=info)
+    assert info["engine"] == "general" and info["status"] == "converged"
+    assert e_ref == pytest.approx(REF[key][0], abs=1e-11)
+    assert e == pytest.approx(REF[key][1], rel=1e-9)
