@@ -89,7 +89,10 @@ __global__ void __launch_bounds__(kThreads) k_prep_ga(nlb_struct_problem P, nlb_
     const int row = ch.hb1 + kq;
     const int q0 = P.fph_ptr[row], q1 = P.fph_ptr[row + 1];
     const T* __restrict__ Bc = static_cast<const T*>(S.t2[c->parity]) + ch.offset;
-    T* __restrict__ Gr = static_cast<T*>(S.g) + ch.ga_off + (int64_t)kq * rowlen;
+    // Ga layout per channel: [b'][k'][i'j'] (the k' values of one (b', i'j')
+    // one hole-pair stride apart, so a reader needs one address per b')
+    const int nhp = ch.nh1 * ch.nh2;
+    T* __restrict__ Gr = static_cast<T*>(S.g) + ch.ga_off + (int64_t)kq * nhp;
     // Ga[k'][e] = sum_c f_ck B[c'][e], the f_ph entries of hole k in order
     constexpr int QR = 8;    // entries kept in registers (a lattice hole has at most six)
     T fv[QR];
@@ -119,7 +122,10 @@ __global__ void __launch_bounds__(kThreads) k_prep_ga(nlb_struct_problem P, nlb_
 #pragma unroll
         for (int r = 0; r < kGaVec; ++r) {
             const int e = e0 + r * (int)blockDim.x;
-            if (e < rowlen) Gr[e] = v[r];
+            if (e < rowlen) {
+                const int bq = e / nhp;
+                Gr[(int64_t)bq * (ch.nh1 - 1) * nhp + e] = v[r];   // (bq * nh1 + kq) * nhp + e % nhp
+            }
         }
     }
 }
@@ -222,11 +228,13 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_t2_rows(nlb_struct_problem P
                     const int col = P.fpp_col[q];
                     acc += (T)P.fpp_val[q] * ((col == ap) ? srow[e] : Bch[(int64_t)col * rowlen + e]);
                 }
+                // Ga[b'][k'][i'j'] of element e = b' * nhp + i'j'
+                const T* ge = Gac + (int64_t)(e / nhp) * (nh1 - 1) * nhp + e;
                 if (NH) {
 #pragma unroll
-                    for (int k = 0; k < (NH ? NH : 1); ++k) acc -= st1a[k] * Gac[(int64_t)k * rowlen + e];
+                    for (int k = 0; k < (NH ? NH : 1); ++k) acc -= st1a[k] * ge[k * nhp];
                 } else {
-                    for (int k = 0; k < nh1; ++k) acc -= st1a[k] * Gac[(int64_t)k * rowlen + e];
+                    for (int k = 0; k < nh1; ++k) acc -= st1a[k] * ge[k * nhp];
                 }
                 sacc[e] = acc;
             }
@@ -581,7 +589,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
         }
         if (active && grp < np2) {
             const T* __restrict__ gB = B + ch.offset + hp;
-            const T* __restrict__ gG = Ga + ch.ga_off + hp;
+            const T* __restrict__ gG = Ga + ch.ga_off + hp;    // Ga[b'][k'][i'j']: k' at stride NHP
             T* __restrict__ Bout = Bo + rbase + hp;
             T* __restrict__ Eout = E2 ? E2 + rbase + hp : nullptr;
             const T* s_hp = srow + hp;
@@ -679,7 +687,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
 #pragma unroll
                 for (int q = 0; q < kLatNa; ++q) rnb[q] = __ldg(gB + aoff[q] + eb);
 #pragma unroll
-                for (int k = 0; k < NH; ++k) rgv[k] = __ldg(gG + k * rowlen + eb);
+                for (int k = 0; k < NH; ++k) rgv[k] = __ldg(gG + eb * NH + k * NHP);
             }
             for (int bp = grp; bp < np2; bp += NB) {
                 const int eb = bp * NHP;
@@ -692,7 +700,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
 #pragma unroll
                 for (int q = 0; q < kLatNa; ++q) rnb[q] = __ldg(gB + aoff[q] + ebn);
 #pragma unroll
-                for (int k = 0; k < NH; ++k) rgv[k] = __ldg(gG + k * rowlen + ebn);
+                for (int k = 0; k < NH; ++k) rgv[k] = __ldg(gG + ebn * NH + k * NHP);
                 element(bp, eb, nb, gv);
             }
             nrm += (double)nrm_row;
@@ -781,8 +789,7 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
                         if (lane == 0) cp[u] = (double)F2[ch.f2_off + (int64_t)ap * ch.nh1 + ip];
                     } else if (ch.g2 == g && lane < ch.nh1) {
                         const int nhp = ch.nh1 * ch.nh2;
-                        const int64_t rowlen = (int64_t)ch.np2 * nhp;
-                        cp[u] = (double)Ga[ch.ga_off + (int64_t)ap * nhp + ip + lane * rowlen + lane * ch.nh2];
+                        cp[u] = (double)Ga[ch.ga_off + ((int64_t)ap * ch.nh1 + lane) * nhp + lane * ch.nh2 + ip];
                     }
                 }
 #pragma unroll
@@ -792,9 +799,8 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
                     const nlb_channel& ch = P.chan[c0 + u];
                     if (ch.g1 != g && ch.g2 == g && ch.nh1 > 16) {
                         const int nhp = ch.nh1 * ch.nh2;
-                        const int64_t rowlen = (int64_t)ch.np2 * nhp;
                         for (int k = lane + 16; k < ch.nh1; k += 16)
-                            part += (double)Ga[ch.ga_off + (int64_t)ap * nhp + ip + k * rowlen + k * ch.nh2];
+                            part += (double)Ga[ch.ga_off + ((int64_t)ap * ch.nh1 + k) * nhp + k * ch.nh2 + ip];
                     }
                 }
             }
