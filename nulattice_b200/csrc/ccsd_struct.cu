@@ -951,60 +951,85 @@ __global__ void __launch_bounds__(kThreads) k_diis_gram(nlb_struct_problem P, nl
 // Leaves in gram[0] the weight of the current amplitudes and in gram[1+s]
 // the weight of error vector s (t_new = w0 t_m + sum_s w_s e_s).
 __global__ void k_diis_solve(nlb_ctrl* c) {
-    if (threadIdx.x != 0 || blockIdx.x != 0 || !c->diis_pulse) return;
+    // one warp: lane t owns column t of the bordered matrix in shared memory;
+    // every entry sees the same operations in the same order as a serial
+    // elimination (partial pivoting, first maximum on ties)
+    if (blockIdx.x != 0 || !c->diis_pulse) return;
+    const int lane = threadIdx.x;
     const int m = c->max_diis, n = m + 1;
-    double A[(kMaxDiis + 1) * (kMaxDiis + 1)], rhs[kMaxDiis + 1];
+    __shared__ double A[kMaxDiis + 1][kMaxDiis + 2];   // column n holds the right-hand side
+    __shared__ double xs[kMaxDiis + 1];
+    __shared__ int s_ok;
     double mx = 0.0;
-    for (int s = 0; s < m; ++s)
-        for (int t = s; t < m; ++t) mx = fmax(mx, fabs(c->gram[s * kMaxDiis + t]));
+    for (int k = lane; k < m * m; k += 32) {
+        const int s = k / m, t = k - s * m;
+        if (t >= s) mx = fmax(mx, fabs(c->gram[s * kMaxDiis + t]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const double nrm = mx + 1e-16;
-    for (int s = 0; s < n; ++s) {
-        rhs[s] = (s == m) ? -1.0 : 0.0;
-        for (int t = 0; t < n; ++t) {
-            double v;
-            if (s < m && t < m) v = c->gram[(s <= t) ? s * kMaxDiis + t : t * kMaxDiis + s] / nrm;
-            else if (s == m && t == m) v = 0.0;
-            else v = -1.0;
-            A[s * n + t] = v;
-        }
+    for (int k = lane; k < n * (n + 1); k += 32) {
+        const int s = k / (n + 1), t = k - s * (n + 1);
+        double v;
+        if (t == n) v = (s == m) ? -1.0 : 0.0;
+        else if (s < m && t < m) v = c->gram[(s <= t) ? s * kMaxDiis + t : t * kMaxDiis + s] / nrm;
+        else if (s == m && t == m) v = 0.0;
+        else v = -1.0;
+        A[s][t] = v;
     }
-    bool ok = true;
-    for (int col = 0; col < n && ok; ++col) {
-        int piv = col;
-        for (int r = col + 1; r < n; ++r)
-            if (fabs(A[r * n + col]) > fabs(A[piv * n + col])) piv = r;
-        if (A[piv * n + col] == 0.0 || !isfinite(A[piv * n + col])) { ok = false; break; }
-        if (piv != col) {
-            for (int t = 0; t < n; ++t) { double tmp = A[col * n + t]; A[col * n + t] = A[piv * n + t]; A[piv * n + t] = tmp; }
-            double tmp = rhs[col]; rhs[col] = rhs[piv]; rhs[piv] = tmp;
+    if (lane == 0) s_ok = 1;
+    __syncwarp();
+    for (int col = 0; col < n; ++col) {
+        if (lane == 0) {
+            int piv = col;
+            for (int r = col + 1; r < n; ++r)
+                if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
+            if (A[piv][col] == 0.0 || !isfinite(A[piv][col])) s_ok = 0;
+            xs[0] = (double)piv;
         }
+        __syncwarp();
+        if (!s_ok) break;
+        const int piv = (int)xs[0];
+        if (piv != col && lane <= n) {
+            const double tmp = A[col][lane]; A[col][lane] = A[piv][lane]; A[piv][lane] = tmp;
+        }
+        __syncwarp();
         for (int r = col + 1; r < n; ++r) {
-            const double f = A[r * n + col] / A[col * n + col];
-            for (int t = col; t < n; ++t) A[r * n + t] -= f * A[col * n + t];
-            rhs[r] -= f * rhs[col];
+            const double f = A[r][col] / A[col][col];
+            __syncwarp();
+            if (lane >= col && lane <= n) A[r][lane] -= f * A[col][lane];
+            __syncwarp();
         }
     }
-    double x[kMaxDiis + 1];
-    if (ok) {
-        for (int r = n - 1; r >= 0; --r) {
-            double s = rhs[r];
-            for (int t = r + 1; t < n; ++t) s -= A[r * n + t] * x[t];
-            x[r] = s / A[r * n + r];
-            if (!isfinite(x[r])) ok = false;
+    __syncwarp();
+    bool ok = s_ok != 0;
+    if (lane == 0) {
+        if (ok) {
+            for (int r = n - 1; r >= 0; --r) {
+                double sum = A[r][n];
+                for (int t = r + 1; t < n; ++t) sum -= A[r][t] * xs[t];
+                xs[r] = sum / A[r][r];
+                if (!isfinite(xs[r])) ok = false;
+            }
         }
-    }
-    c->diis_applied = ok ? 1 : 0;
-    if (!ok) return;
-    // t_new = sum_k x_k t_{k+1},  t_{k+1} = t_m - sum_{s>k} e_s
-    double tot = 0.0;
-    for (int k = 0; k < m; ++k) tot += x[k];
-    c->gram[0] = tot;
-    double run = 0.0;
-    for (int s = 0; s < m; ++s) {
-        c->gram[1 + s] = -run;
-        run += x[s];
+        c->diis_applied = ok ? 1 : 0;
+        if (ok) {
+            // t_new = sum_k x_k t_{k+1},  t_{k+1} = t_m - sum_{s>k} e_s
+            double tot = 0.0;
+            for (int k = 0; k < m; ++k) tot += xs[k];
+            c->gram[0] = tot;
+            double run = 0.0;
+            for (int s = 0; s < m; ++s) {
+                c->gram[1 + s] = -run;
+                run += xs[s];
+            }
+        }
     }
 }
+
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
 
 template <typename T, int M>
 __global__ void __launch_bounds__(kThreads) k_diis_extrap(nlb_struct_problem P, nlb_struct_state S) {
@@ -1021,19 +1046,40 @@ __global__ void __launch_bounds__(kThreads) k_diis_extrap(nlb_struct_problem P, 
     T* t2 = static_cast<T*>(S.t2[par]);
     const T* E2 = static_cast<const T*>(S.diis_t2);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n1 + n2; e += stride) {
-        if (e < n1) {
-            double v = w0 * t1[e];
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t e = tid; e < n1; e += stride) {
+        double v = w0 * t1[e];
 #pragma unroll
-            for (int s = 0; s < M; ++s) v += w[s] * S.diis_t1[(int64_t)s * n1 + e];
-            t1[e] = v;
-        } else {
-            const int64_t q = e - n1;
-            double v = w0 * (double)t2[q];
+        for (int s = 0; s < M; ++s) v += w[s] * S.diis_t1[(int64_t)s * n1 + e];
+        t1[e] = v;
+    }
+    // T2: two amplitudes per thread with 8- (FP32) or 16-byte (FP64) loads
+    // when every stored vector starts on such a boundary (n_t2 even, aligned
+    // buffers); the arithmetic per amplitude is the same as one at a time
+    using V = typename Vec2<T>::type;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(t2) | reinterpret_cast<uintptr_t>(E2)) % sizeof(V)) == 0;
+    const int64_t npair = (P.n_t2 % 2 == 0 && aligned) ? n2 / 2 : 0;
+    V* t2v = reinterpret_cast<V*>(t2);
+    const V* E2v = reinterpret_cast<const V*>(E2);
+    for (int64_t q = tid; q < npair; q += stride) {
+        const V a = t2v[q];
+        double vx = w0 * (double)a.x, vy = w0 * (double)a.y;
 #pragma unroll
-            for (int s = 0; s < M; ++s) v += w[s] * (double)E2[(int64_t)s * P.n_t2 + q];
-            t2[q] = (T)v;
+        for (int s = 0; s < M; ++s) {
+            const V b = E2v[(int64_t)s * (P.n_t2 / 2) + q];
+            vx += w[s] * (double)b.x;
+            vy += w[s] * (double)b.y;
         }
+        V o;
+        o.x = (T)vx;
+        o.y = (T)vy;
+        t2v[q] = o;
+    }
+    for (int64_t q = 2 * npair + tid; q < n2; q += stride) {
+        double v = w0 * (double)t2[q];
+#pragma unroll
+        for (int s = 0; s < M; ++s) v += w[s] * (double)E2[(int64_t)s * P.n_t2 + q];
+        t2[q] = (T)v;
     }
 }
 
@@ -1269,7 +1315,7 @@ void diis_m(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t
     const int64_t n = (int64_t)P->p * P->h + P->n_t2;
     k_diis_gram<T, M><<<grid_for(k_diis_gram<T, M>, n), kThreads, 0, st>>>(*P, *S);
     k_diis_solve<<<1, 32, 0, st>>>(S->ctrl);
-    k_diis_extrap<T, M><<<grid_for(k_diis_extrap<T, M>, n), kThreads, 0, st>>>(*P, *S);
+    k_diis_extrap<T, M><<<grid_for(k_diis_extrap<T, M>, (n + 1) / 2), kThreads, 0, st>>>(*P, *S);
     k_diis_done<<<1, 32, 0, st>>>(S->ctrl);
 }
 
