@@ -289,12 +289,10 @@ def main():
     clocks = clk.summary()
     d_ms, d_k, d_info, d_e, _ = timed("fp64")
 
+    from nulattice_b200 import batch as B
+
     def gmax(x):
-        if ws > 1:
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return B.max_over_ranks(x, dev)
 
     tts_mixed = gmax(statistics.mean(m_ms)) / 1e3
     tts_fp64 = gmax(statistics.mean(d_ms)) / 1e3
@@ -389,11 +387,7 @@ def batch_leg(dev, peak_gbs, rank=0, ws=1):
     t_batch = statistics.median(times)
 
     def gmax(x):
-        if ws > 1:
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return B.max_over_ranks(x, dev)
     t_batch = gmax(t_batch)
     res = scan.results()
     ok = [r for r in res if r["status"] == "converged" and r["lambda_status"] == "converged"]
@@ -432,8 +426,7 @@ def batch_leg(dev, peak_gbs, rank=0, ws=1):
                               abs(2 * g[1] - r["dE_dC3"]) / abs(r["dE_dC3"])))
     scan.close()
     if ws > 1:
-        gathered = [None] * ws
-        torch.distributed.all_gather_object(gathered, (res, failed, diffs, alg))
+        gathered = B.gather_results([(res, failed, diffs, alg)])
         res = [r for g in gathered for r in g[0]]
         failed = [f for g in gathered for f in g[1]]
         diffs = [d for g in gathered for d in g[2]]

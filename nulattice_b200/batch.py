@@ -67,6 +67,31 @@ def shard(instances, rank, world):
     return [instances[i] for i in range(len(instances)) if owner[i] == rank]
 
 
+def max_over_ranks(x, device=None):
+    """The largest value of ``x`` over the ranks of the default process group
+    (the job's time is the slowest rank's); ``x`` itself without one.  NCCL
+    groups reduce on ``device`` (the rank's GPU), others on the CPU."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    if device is None:
+        device = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gather_results(local):
+    """Every rank's list of per-instance results, concatenated in rank order
+    (one ``all_gather_object``); ``local`` itself without a process group."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(local)
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, list(local))
+    return [r for p in parts for r in p]
+
+
 def combine(parts, coeffs):
     """sum_k c_k H_k of builder outputs (E_ref, fock, two-body blocks); sparse
     blocks are concatenated (repeated keys are summed downstream)."""
