@@ -323,6 +323,14 @@ typedef struct {
 int nlb_contract_f64(const nlb_contract_desc *d, const double *A, const double *B, double *C,
                      double alpha, double beta, nlb_stream_t stream);
 
+/* The same contraction (no batch indices) as one library GEMM: A and B are
+ * gathered into row-major [M][K] and [K][N] panels in `work`, multiplied by
+ * cublasDgemm on `stream` and written back into the strided C (alpha, beta as
+ * above).  `work` holds nlb_contract_gemm_work(d) bytes. */
+int64_t nlb_contract_gemm_work(const nlb_contract_desc *d);
+int nlb_contract_gemm_f64(const nlb_contract_desc *d, const double *A, const double *B, double *C,
+                          double alpha, double beta, double *work, int64_t work_bytes, nlb_stream_t stream);
+
 /* H += alpha * P(Z) on (p,p,h,h) tensors, P = 1, pAB, pIJ or pIJ pAB
  * (perm 0..3; ccDgrams.py:193-213). */
 int nlb_antisym_acc_f64(const double *Z, double *H, int64_t p, int64_t h, int32_t perm,

@@ -132,6 +132,10 @@ def lib():
         getattr(L, name).restype = c_int32
     L.nlb_contract_f64.argtypes = [ctypes.POINTER(ContractDesc), c_void_p, c_void_p, c_void_p, c_double, c_double,
                                    c_void_p]
+    L.nlb_contract_gemm_work.argtypes = [ctypes.POINTER(ContractDesc)]
+    L.nlb_contract_gemm_work.restype = c_int64
+    L.nlb_contract_gemm_f64.argtypes = [ctypes.POINTER(ContractDesc), c_void_p, c_void_p, c_void_p, c_double,
+                                        c_double, c_void_p, c_int64, c_void_p]
     L.nlb_antisym_acc_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int64, c_int32, c_double, c_void_p]
     L.nlb_ppph_intermediates_f64.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_int64,
                                              c_void_p, c_void_p]

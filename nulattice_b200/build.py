@@ -29,7 +29,7 @@ def build(force=False, verbose=False):
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest:
         return OUT
     cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-o", OUT + ".tmp", *srcs]
+           "-I", os.path.join(ROOT, "include"), "-o", OUT + ".tmp", *srcs, "-lcublas"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -10,6 +10,7 @@
 // antisymmetrisers pAB / pIJ are folded into one accumulate kernel, and the
 // Jacobi update, energy and DIIS are fused elementwise kernels.
 
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -367,6 +368,47 @@ int grid1(int64_t n) {
     return (int)(g < 4096 ? (g > 0 ? g : 1) : 4096);
 }
 
+// Packing for the GEMM path of a contraction: X[r * cols + c] =
+// src[decode(r) + decode(c)] (row-major panels the library GEMM reads), and
+// the strided write-back C = alpha * P + beta * C.
+__global__ void k_pack(const double* __restrict__ src, double* __restrict__ dst, int64_t rows, int64_t cols,
+                       nlb_contract_desc d, int which) {
+    const int64_t n = rows * cols;
+    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = l / cols, c = l - r * cols;
+        int64_t off;
+        if (which == 0) off = decode(r, d.ext_m, d.sa_m, d.nm) + decode(c, d.ext_k, d.sa_k, d.nk);   // A[m][k]
+        else off = decode(r, d.ext_k, d.sb_k, d.nk) + decode(c, d.ext_n, d.sb_n, d.nn);              // B[k][n]
+        dst[l] = src[off];
+    }
+}
+
+__global__ void k_unpack_c(const double* __restrict__ P, double* __restrict__ C, nlb_contract_desc d, double alpha,
+                           double beta) {
+    const int64_t n = d.M * d.N;
+    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = l / d.N, q = l - m * d.N;
+        const int64_t off = decode(m, d.ext_m, d.sc_m, d.nm) + decode(q, d.ext_n, d.sc_n, d.nn);
+        const double v = alpha * P[l];
+        C[off] = (beta == 0.0) ? v : v + beta * C[off];
+    }
+}
+
+// One cuBLAS handle per device, bound to the caller's stream at each call.
+cublasHandle_t g_blas[64] = {};
+
+cublasHandle_t blas_handle(cudaStream_t st) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!g_blas[dev] && cublasCreate(&g_blas[dev]) != CUBLAS_STATUS_SUCCESS) {
+        g_blas[dev] = nullptr;
+        return nullptr;
+    }
+    if (cublasSetStream(g_blas[dev], st) != CUBLAS_STATUS_SUCCESS) return nullptr;
+    return g_blas[dev];
+}
+
 }  // namespace
 
 extern "C" {
@@ -387,6 +429,40 @@ int nlb_contract_f64(const nlb_contract_desc* d, const double* A, const double* 
         k_contract<<<grid, 256, 0, (cudaStream_t)stream>>>(*d, A, B, C, alpha, beta);
     }
     return dcheck("nlb_contract_f64");
+}
+
+int64_t nlb_contract_gemm_work(const nlb_contract_desc* d) {
+    if (!d) return 0;
+    return (d->M * d->K + d->K * d->N + d->M * d->N) * (int64_t)sizeof(double);
+}
+
+int nlb_contract_gemm_f64(const nlb_contract_desc* d, const double* A, const double* B, double* C, double alpha,
+                          double beta, double* work, int64_t work_bytes, nlb_stream_t stream) {
+    if (!d || !A || !B || !C || !work) return dfail(NLB_ERR_ARG, "nlb_contract_gemm_f64: null argument");
+    if (d->nm > 4 || d->nn > 4 || d->nk > 4 || d->nm < 0 || d->nn < 0 || d->nk < 0 || d->nb != 0 || d->B != 1)
+        return dfail(NLB_ERR_ARG, "nlb_contract_gemm_f64: no batch indices, at most 4 indices per group");
+    if (d->M <= 0 || d->N <= 0) return NLB_OK;
+    if (d->K <= 0) return nlb_contract_f64(d, A, B, C, alpha, beta, stream);
+    if (work_bytes < nlb_contract_gemm_work(d)) return dfail(NLB_ERR_SIZE, "nlb_contract_gemm_f64: workspace too small");
+    if (d->M > 0x7fffffff || d->N > 0x7fffffff || d->K > 0x7fffffff)
+        return dfail(NLB_ERR_SIZE, "nlb_contract_gemm_f64: a GEMM side exceeds 2^31");
+    cudaStream_t st = (cudaStream_t)stream;
+    double* Ap = work;
+    double* Bp = Ap + d->M * d->K;
+    double* Cp = Bp + d->K * d->N;
+    k_pack<<<grid1(d->M * d->K), 256, 0, st>>>(A, Ap, d->M, d->K, *d, 0);
+    k_pack<<<grid1(d->K * d->N), 256, 0, st>>>(B, Bp, d->K, d->N, *d, 1);
+    int rc = dcheck("nlb_contract_gemm_f64 (pack)");
+    if (rc != NLB_OK) return rc;
+    cublasHandle_t hb = blas_handle(st);
+    if (!hb) return dfail(NLB_ERR_LAUNCH, "nlb_contract_gemm_f64: cuBLAS handle");
+    // row-major Cp[M][N] = Ap[M][K] Bp[K][N]  <=>  column-major Cp^T = Bp^T Ap^T
+    const double one = 1.0, zero = 0.0;
+    if (cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, (int)d->N, (int)d->M, (int)d->K, &one, Bp, (int)d->N, Ap,
+                    (int)d->K, &zero, Cp, (int)d->N) != CUBLAS_STATUS_SUCCESS)
+        return dfail(NLB_ERR_LAUNCH, "nlb_contract_gemm_f64: cublasDgemm failed");
+    k_unpack_c<<<grid1(d->M * d->N), 256, 0, st>>>(Cp, C, *d, alpha, beta);
+    return dcheck("nlb_contract_gemm_f64 (write-back)");
 }
 
 int nlb_antisym_acc_f64(const double* Z, double* H, int64_t p, int64_t h, int32_t perm, double alpha,

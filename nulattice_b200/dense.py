@@ -75,14 +75,22 @@ TERMS = {
 }
 
 
+# contractions with at least this many multiply-adds (and no batch index)
+# go through gathered panels and one library GEMM (FP64 tensor cores)
+GEMM_MIN_MACS = 1 << 18
+
+
 class GpuEinsum:
-    """Einsum over CUDA FP64 tensors through ``nlb_contract_f64``."""
+    """Einsum over CUDA FP64 tensors through ``nlb_contract_f64`` (strided
+    tiles) or, for large contractions, ``nlb_contract_gemm_f64``."""
 
     def __init__(self, stream_ptr):
         self.L = _lib.lib()
         self.sp = ctypes.c_void_p(stream_ptr)
         self._plans = {}
+        self._ws = None
         self.launches = 0
+        self.gemms = 0
 
     # -- one pairwise contraction ------------------------------------------
     def pair(self, spec, A, B, out, alpha=1.0, beta=0.0):
@@ -127,6 +135,17 @@ class GpuEinsum:
                     d.sa_b[q] = sa[x]; d.sb_b[q] = sb[x]; d.sc_b[q] = sc[x]
         prod = lambda g: int(np.prod([ext[x] for x in groups[g]])) if groups[g] else 1  # noqa: E731
         d.M, d.N, d.K, d.B = prod("m"), prod("n"), prod("k"), prod("b")
+        if d.B == 1 and d.K > 0 and d.M * d.N * d.K >= GEMM_MIN_MACS:
+            # large contractions: gathered panels and one library GEMM
+            need = int(self.L.nlb_contract_gemm_work(ctypes.byref(d)))
+            if self._ws is None or self._ws.numel() * 8 < need:
+                self._ws = torch.empty((need + 7) // 8, dtype=torch.float64, device=out.device)
+            _lib.check(self.L.nlb_contract_gemm_f64(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
+                                                    alpha, beta, self._ws.data_ptr(), self._ws.numel() * 8,
+                                                    self.sp), "contract (gemm)")
+            self.launches += 4
+            self.gemms += 1
+            return
         _lib.check(self.L.nlb_contract_f64(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
                                            alpha, beta, self.sp), "contract")
         self.launches += 1

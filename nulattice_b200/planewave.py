@@ -19,8 +19,8 @@ shells, in the input layout of :func:`nulattice_b200.ccsd.ccsd_solver`:
 * three-body ``<ijk||lmn> = w3 sgn(perm) / L^6`` when the spin-isospin labels
   of the ket are a permutation of the bra's (all distinct) and the momenta
   add up.  With every hole momentum filled in all four spin-isospin states
-  its normal-ordered parts are, for ``n_k`` hole momenta: ``E_3 = 4 n_k^3
-  ... = (1/6) #(ordered hole triples with distinct labels) w3 / L^6``,
+  its normal-ordered parts are, for ``n_k`` hole momenta: ``E_3 = (1/6)
+  #(ordered hole triples with distinct labels) w3 / L^6 = 4 n_k^3 w3 / L^6``,
   ``f_3 = (1/2) #(ordered hole pairs with labels distinct from each other and
   from the state) w3 / L^6`` on the diagonal, and a two-body part equal to an
   SU(4) contact of strength ``2 n_k w3 / L^3`` (the sums of
@@ -79,9 +79,14 @@ def _vloc_tensor(vT1, vS1):
     return v
 
 
-def two_body_rows(vT1, vS1, L):
+def two_body_rows(vT1, vS1, L, k_full=None, is_hole=None):
     """Rows ``[p, q, r, s, <pq||rs>]`` (p<q, r<s) of the contact in the
-    plane-wave basis: momentum conservation modulo L, value ``v_loc / L^3``."""
+    plane-wave basis: momentum conservation modulo L, value ``v_loc / L^3``.
+
+    ``k_full`` (bool per total momentum K, with ``is_hole`` per state): at
+    the K where it is False only rows whose bra and ket pairs both hold a
+    hole are emitted (the p-h blocks need every K; the pure-particle and
+    three-particle rows there only ever meet amplitudes that vanish)."""
     n = 4 * L ** 3
     v = _vloc_tensor(vT1, vS1) / L ** 3
     i, j = np.triu_indices(n, 1)
@@ -100,6 +105,8 @@ def two_body_rows(vT1, vS1, L):
     rows = []
     for k in range(L ** 3):
         sel = order[bounds[k]:bounds[k + 1]]
+        if k_full is not None and not k_full[k]:
+            sel = sel[is_hole[i[sel]] | is_hole[j[sel]]]
         if len(sel) == 0:
             continue
         a, b = i[sel], j[sel]
@@ -121,13 +128,15 @@ def kinetic_rows(L):
     return np.stack([s, s, t], 1).astype(np.float64)
 
 
-def plane_wave_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True):
+def plane_wave_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True, prune=True):
     """Normal-ordered plane-wave Hamiltonian, returned like
     :func:`hamiltonian.normal_ordered_hamiltonian`:
     ``(E_ref, [f_pp, f_ph, f_hh], [v_pppp, v_ppph, v_pphh, v_phph, v_phhh, v_hhhh])``.
 
     ``holes`` are ``[nx, ny, nz, tz, sz]`` rows (:func:`momentum_holes`);
-    every hole momentum must hold all four spin-isospin states."""
+    every hole momentum must hold all four spin-isospin states.  ``prune``
+    leaves out the v_pppp / v_ppph rows at total momenta no hole pair has
+    (they never meet a non-zero amplitude; ``prune=False`` keeps every row)."""
     holes = np.asarray(holes, dtype=np.int64).reshape(-1, 5)
     hole, part = _ham.ph_split(holes, L)
     h, p = len(hole), len(part)
@@ -142,11 +151,23 @@ def plane_wave_hamiltonian(L, holes, vT1, vS1, w3=0.0, dense=True):
     loc = np.zeros(n, np.int64); loc[hole] = np.arange(h); loc[part] = np.arange(p)
 
     shapes = {"pphh": (p, p, h, h), "phph": (p, h, p, h), "phhh": (p, h, h, h), "hhhh": (h, h, h, h)}
-    b = _ham._sort_two_body(two_body_rows(vT1, vS1, L), is_hole, loc)
+    # Closed shells: every hole momentum is full, so t1 vanishes by momentum
+    # conservation and t2[a,b,i,j] lives at the total momenta K of hole
+    # pairs.  v_pppp and v_ppph rows at any other K only multiply vanishing
+    # amplitudes, and are left out (exact: their products are zeros).
+    kfull = np.zeros(L ** 3, bool)
+    hkeys = list(hk)
+    for k1 in hkeys:
+        for k2 in hkeys:
+            kk = [(k1[d] + k2[d]) % L for d in range(3)]
+            kfull[(kk[0] * L + kk[1]) * L + kk[2]] = True
+    if not prune:
+        kfull[:] = True
+    b = _ham._sort_two_body(two_body_rows(vT1, vS1, L, kfull, is_hole), is_hole, loc)
     # normal-ordered three-body part: an SU(4) contact of strength 2 n_k w3 / L^3
     if w3 != 0.0:
         v3 = 2.0 * n_k * w3 / L ** 3
-        b3 = _ham._sort_two_body(two_body_rows(v3, v3, L), is_hole, loc)
+        b3 = _ham._sort_two_body(two_body_rows(v3, v3, L, kfull, is_hole), is_hole, loc)
         # E_3 and the diagonal f_3 from the counts of distinct-label hole tuples
         n_h = 4 * n_k
         e3 = (n_h * (n_h - n_k) * (n_h - 2 * n_k)) / 6.0 * w3 / L ** 6

@@ -93,3 +93,33 @@ def test_pulsed_diis_general_engine():
         e, t1, t2 = ccsd_solver(fock, two, eps=0.0, maxSteps=steps, max_diis=4, device=DEV, engine="general")
         assert e == pytest.approx(float(d[f"diis_e_{steps}"]), rel=1e-11)
         np.testing.assert_allclose(t1, d[f"diis_t1_{steps}"], atol=1e-11)
+
+
+@pytest.mark.parametrize("spec,shapes", [
+    ("bkcj,acik->abij", {"a": 40, "b": 40, "c": 40, "i": 6, "j": 6, "k": 6}),     # ring term
+    ("klcd,cdij->klij", {"c": 48, "d": 48, "i": 5, "j": 5, "k": 5, "l": 5}),      # pp-ladder shape
+    ("aick,bjck->abij", {"a": 33, "b": 31, "c": 29, "i": 4, "j": 4, "k": 4}),     # ragged extents
+])
+@pytest.mark.parametrize("beta", [0.0, 0.7])
+def test_gemm_path_matches_strided_kernel(monkeypatch, spec, shapes, beta):
+    """The gathered-panel library GEMM gives the strided contraction kernel's
+    result (alpha, beta and permuted operand strides included)."""
+    g = torch.Generator().manual_seed(5)
+    ins, oz = spec.split("->")
+    ta, tb = ins.split(",")
+    A = torch.randn([shapes[x] for x in ta], generator=g, dtype=torch.float64).to(DEV)
+    B = torch.randn([shapes[x] for x in tb], generator=g, dtype=torch.float64).to(DEV)
+    B = B.transpose(0, 2).contiguous().transpose(0, 2)          # non-contiguous strides
+    C0 = torch.randn([shapes[x] for x in oz], generator=g, dtype=torch.float64).to(DEV)
+    outs = []
+    for min_macs in (1 << 62, 1):
+        monkeypatch.setattr(D, "GEMM_MIN_MACS", min_macs)
+        E = D.GpuEinsum(torch.cuda.current_stream(DEV).cuda_stream)
+        C = C0.clone()
+        E.pair(spec, A, B, C, alpha=-0.5, beta=beta)
+        outs.append((C.cpu().numpy(), E.gemms))
+    (c_tile, n0), (c_gemm, n1) = outs
+    assert n0 == 0 and n1 == 1
+    ref = -0.5 * np.einsum(spec, A.cpu().numpy(), B.cpu().numpy()) + beta * C0.cpu().numpy()
+    np.testing.assert_allclose(c_tile, ref, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(c_gemm, ref, rtol=1e-12, atol=1e-12)

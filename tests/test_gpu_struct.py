@@ -222,3 +222,15 @@ def test_plane_wave_inputs_match_reference(key):
     assert info["engine"] == "general" and info["status"] == "converged"
     assert e_ref == pytest.approx(REF[key][0], abs=1e-11)
     assert e == pytest.approx(REF[key][1], rel=1e-9)
+
+
+def test_plane_wave_L4_steps_match_oracle():
+    """Plane waves at L=4 (beyond what the reference solves in minutes):
+    five Jacobi steps of the general engine against the oracle."""
+    from nulattice_b200 import planewave as PW
+    e_ref, fock, two = PW.plane_wave_hamiltonian(4, PW.momentum_holes(4, 4), -3.0, -3.0, 1.0, dense=False)
+    e, t1, t2 = ccsd_solver(fock, two, eps=0.0, maxSteps=5, max_diis=0, device=DEV, criterion="numpy")
+    dense_two = [two[0], two[1]] + [b.to_dense() for b in two[2:]]
+    eo, t1o, t2o, it, st = O.solve(fock, dense_two, eps=0.0, maxSteps=5, max_diis=0, criterion="numpy")
+    assert e == pytest.approx(eo, rel=1e-12)
+    np.testing.assert_allclose(t2, t2o, rtol=0, atol=1e-12 * np.abs(t2o).max())

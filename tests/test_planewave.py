@@ -79,3 +79,18 @@ def test_oracle_reproduces_reference_L2():
     res = O.solve(f, two, eps=1e-13, maxSteps=3000, max_diis=10)
     assert res[4] == "converged"
     assert res[0] == pytest.approx(REF[(L, v, w)][1], rel=1e-10)
+
+
+@pytest.mark.parametrize("L,A,w,steps", [(2, 4, 1.0, 4), (3, 4, 1.0, 4), (3, 28, 0.5, 1)])
+def test_pruned_rows_change_nothing(L, A, w, steps):
+    """Leaving out the v_pppp / v_ppph rows at total momenta no hole pair
+    has gives bit for bit the same solve (they only meet zero amplitudes)."""
+    from oracle import ccsd_oracle as O
+    out = []
+    for prune in (True, False):
+        e, f, two = PW.plane_wave_hamiltonian(L, PW.momentum_holes(L, A), -3.0, -3.0, w, prune=prune)
+        r = O.solve(f, two, eps=0.0, maxSteps=steps, max_diis=0)
+        out.append((e, r[0], r[2], len(two[0])))
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    np.testing.assert_array_equal(out[0][2], out[1][2])
+    assert out[0][3] < out[1][3]
