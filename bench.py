@@ -178,7 +178,8 @@ def run_reference(args):
            "warmup": args.warmup, "ms_per_step": s_iter * 1e3, "higher_is_better": False,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
            "data": "synthetic lattice Hamiltonian built in-process",
-           "config": {"workload": "ccsd_L6_A28", "L": L_BENCH, "A": A_BENCH, "C2": C2, "C3": C3},
+           "config": {"workload": "ccsd_L6_A28_mixed", "L": L_BENCH, "A": A_BENCH, "C2": C2, "C3": C3,
+                      "path": "the reference's CPU algorithm (FP64 Jacobi + mixing, every diagram)"},
            "cpu_baseline": {"value": val, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
            "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
