@@ -75,6 +75,9 @@ TERMS = {
 }
 
 
+# a 4-D v_pppp with at least this fraction non-zero stays dense (ladders as GEMMs)
+DENSE_PPPP_FRACTION = 8
+
 # contractions with at least this many multiply-adds (and no batch index)
 # go through gathered panels and one library GEMM (FP64 tensor cores)
 GEMM_MIN_MACS = 1 << 18
@@ -200,13 +203,17 @@ class GpuEinsum:
 
 
 def _dense_block(x, shape, dev):
+    """A C-contiguous FP64 copy on ``dev``: the element-wise kernels (Jacobi,
+    antisymmetrisers, energy) index the blocks and every tensor cloned from
+    them in row-major order, whatever the strides of the caller's array
+    (``np.einsum`` and transposes return permuted strides)."""
     if x is None:
         return torch.zeros(shape, dtype=torch.float64, device=dev)
     if isinstance(x, torch.Tensor):
         return x.to(device=dev, dtype=torch.float64).contiguous()
     if hasattr(x, "to_dense"):
-        return torch.as_tensor(np.asarray(x.to_dense(), dtype=np.float64), device=dev)
-    return torch.as_tensor(np.asarray(x, dtype=np.float64), device=dev)
+        x = x.to_dense()
+    return torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device=dev)
 
 
 def _rows_dev(x, dev):
@@ -241,7 +248,14 @@ class DenseEngine:
         # onto antisymmetric tensors (see nlb_antisym_project_f64).
         v = self.T["v_pphh"]
         self.antisym = bool(torch.equal(v, -v.permute(1, 0, 2, 3)) and torch.equal(v, -v.permute(0, 1, 3, 2)))
-        self.pppp = self._sparse(v_pppp, (p, p, p, p))
+        # a dense v_pppp (a rotated, e.g. Hartree-Fock, basis) keeps its dense
+        # form: both ladders are then GEMM-shaped contractions
+        self.pppp_dense = None
+        if isinstance(v_pppp, (np.ndarray, torch.Tensor)) and v_pppp.ndim == 4:
+            vd = _dense_block(v_pppp, (p, p, p, p), dev)
+            if int(torch.count_nonzero(vd).item()) * DENSE_PPPP_FRACTION >= vd.numel():
+                self.pppp_dense = vd
+        self.pppp = self._sparse(v_pppp, (p, p, p, p)) if self.pppp_dense is None else (None, None, 0)
         self.ppph = self._sparse(v_ppph, (p, p, p, h))
         self.stream = torch.cuda.current_stream(dev)
         self.E = GpuEinsum(self.stream.cuda_stream)
@@ -330,12 +344,17 @@ class DenseEngine:
             _lib.check(self.L.nlb_antisym_acc_f64(r[2].data_ptr(), h2.data_ptr(), p, h, 2, 1.0, self.sp), "pij")
             for n in ("dgram_da_dbij", "dgram_acik_bcjk", "dgram_bijk_ak1", "dgram_bijk_ak2"):
                 self._term(n, ops, h2, tmp)
-        if self.pppp[2]:
+        if self.pppp[2] or self.pppp_dense is not None:
             l1 = torch.zeros((p, p, h, h), dtype=torch.float64, device=dev)
             l2 = torch.zeros((p, p, h, h), dtype=torch.float64, device=dev)
-            _lib.check(self.L.nlb_pppp_ladders_f64(self.pppp[0].data_ptr(), self.pppp[1].data_ptr(), self.pppp[2],
-                                                   t1.data_ptr(), t2.data_ptr(), p, h, l1.data_ptr(),
-                                                   l2.data_ptr(), self.sp), "pppp")
+            if self.pppp_dense is not None:
+                # the same sums as the list kernel: l1 = v t2, l2 = v (t1 x t1)
+                self.E("abcd,cdij->abij", self.pppp_dense, t2, out=l1)
+                self.E("abcd,ci,dj->abij", self.pppp_dense, t1, t1, out=l2)
+            else:
+                _lib.check(self.L.nlb_pppp_ladders_f64(self.pppp[0].data_ptr(), self.pppp[1].data_ptr(),
+                                                       self.pppp[2], t1.data_ptr(), t2.data_ptr(), p, h,
+                                                       l1.data_ptr(), l2.data_ptr(), self.sp), "pppp")
             _lib.check(self.L.nlb_antisym_acc_f64(l1.data_ptr(), h2.data_ptr(), p, h, 0, 0.5, self.sp), "l1")
             _lib.check(self.L.nlb_antisym_acc_f64(l2.data_ptr(), h2.data_ptr(), p, h, 2, 0.5, self.sp), "l2")
         self.E("bc,acij->abij", xpp2, t2, out=tmp)

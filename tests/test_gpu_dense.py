@@ -149,3 +149,24 @@ def test_reproduces_reference_table5(key):
         assert info["engine"] == engine
         mev = (e + e_ref) * ham.phys_unit(a_lat)
         assert abs(mev - want) <= 0.005 + 1e-9, (key, holes == HE3, mev, want)
+
+
+@pytest.mark.parametrize("holes", ["he4", "he3"])
+def test_rotated_dense_inputs(holes):
+    """A basis rotated within the particles and within the holes (as after
+    Hartree-Fock): every non-zero block dense, v_pppp as a dense 4-D array
+    (its ladders as library GEMMs).  The correlation energy equals the one
+    of the unrotated input -- for the closed-site 4He that one comes from the
+    structured engine, so the two engines check each other."""
+    import rotation
+    from nulattice_b200 import hamiltonian as ham
+    hl = ham.closed_shell_holes(2, 4) if holes == "he4" else HE3
+    e_ref, fock, two = ham.normal_ordered_hamiltonian(2, hl, -6.0, -6.0, 2.0)
+    fr, tr = rotation.rotate(fock, two, 3)
+    i0, i1 = {}, {}
+    e0, _, _ = ccsd_solver(fock, two, eps=1e-12, maxSteps=3000, max_diis=8, device=DEV, info=i0)
+    e1, _, _ = ccsd_solver(fr, tr, eps=1e-12, maxSteps=3000, max_diis=8, device=DEV, info=i1)
+    assert i1["engine"] == "general"
+    assert i0["engine"] == ("structured" if holes == "he4" else "general")
+    assert i0["status"] == "converged" and i1["status"] == "converged"
+    assert e1 == pytest.approx(e0, rel=1e-9)

@@ -2,6 +2,7 @@
 import ctypes
 
 import numpy as np
+import torch
 import pytest
 
 import golden_io as G
@@ -186,3 +187,16 @@ def test_batch_shards_are_disjoint_complete_and_balanced():
         biggest = max(B.instance_cost(a, l) for a, l, _, _ in inst)
         assert max(loads) - min(loads) <= biggest
     assert B.instance_cost(28, 6) == 6 * 209 * 209 * 49
+
+
+def test_dense_blocks_are_row_major_whatever_the_input_strides():
+    """The general engine's element-wise kernels index its blocks (and the
+    residuals cloned from them) in row-major order: a block handed over with
+    permuted strides, as np.einsum returns them, is stored row-major."""
+    from nulattice_b200 import dense as Dn
+    x = np.random.default_rng(1).standard_normal((3, 4, 2, 5))
+    for y in (x.transpose(2, 0, 3, 1), np.einsum("abcd->dcba", x, optimize=True), x[:, ::2]):
+        t = Dn._dense_block(y, None, "cpu")
+        assert t.is_contiguous() and t.dtype.is_floating_point
+        np.testing.assert_array_equal(t.numpy(), y)
+        assert Dn._dense_block(torch.as_tensor(y), None, "cpu").is_contiguous()

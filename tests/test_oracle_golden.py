@@ -86,3 +86,23 @@ def test_pulsed_diis_matches_torch_solver():
 def test_fixed_point_gap_small_at_golden():
     g = G.load("he4_L3_c1")
     assert max(g["tight_gap"]) < 1e-12
+
+
+HE3 = [[0, 0, 0, 0, 0], [0, 0, 0, 1, 0], [0, 0, 0, 0, 1]]
+
+
+@pytest.mark.parametrize("holes", ["he4"])
+def test_rotation_invariance_of_the_oracle(holes):
+    """Rotating particles and holes separately makes every non-zero block
+    dense but leaves the CCSD correlation energy unchanged (the premise of
+    the GPU test of dense, rotated-basis inputs)."""
+    import rotation
+    from nulattice_b200 import hamiltonian as ham
+    hl = ham.closed_shell_holes(2, 4) if holes == "he4" else HE3
+    e_ref, fock, two = ham.normal_ordered_hamiltonian(2, hl, -6.0, -6.0, 2.0)
+    fr, tr = rotation.rotate(fock, two, 3)
+    assert np.count_nonzero(tr[0]) > 0.5 * tr[0].size and np.count_nonzero(fr[0]) > 0.5 * fr[0].size
+    e0 = O.solve(fock, two, eps=1e-13, maxSteps=3000, max_diis=8)[0]
+    e1 = O.solve(fr, [rotation.rows_of(tr[0]), rotation.rows_of(tr[1])] + tr[2:], eps=1e-13, maxSteps=3000,
+                 max_diis=8)[0]
+    assert e1 == pytest.approx(e0, rel=1e-9)
