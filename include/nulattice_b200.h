@@ -370,6 +370,64 @@ int nlb_dense_energy_f64(const double *f_ph, const double *t1, const double *v_p
 int nlb_vec_diis_f64(const double *err, const double *hist, int64_t n, int32_t m, double *work,
                      double *out, nlb_stream_t stream);
 
+/* ------------------------------------------------------------------------
+ * Momentum-block path: closed-shell plane-wave inputs with a contact
+ * interaction (the input family of planewave.py, fed to the reference's
+ * ccsd_solver at CCM/coupled_cluster.py:547-687).  Every hole momentum holds
+ * all four spin-isospin states, so t1 vanishes by momentum conservation and
+ * t2[a,b,i,j] lives in blocks of total momentum K = k_a + k_b = k_i + k_j:
+ * block b is a row-major [nr x nc] matrix, row = pa*16 + s_a*4 + s_b (pa the
+ * position of k_a among the block's particle momenta), col = pi*16 + s_i*4 +
+ * s_j.  The interaction is <pq||rs> = V[s_p s_q s_r s_s] delta(K).  The
+ * residual is the T2 equation of coupled_cluster.py:476-536 at t1 = 0
+ * (ccDgrams.py:215-303, 502-527), the step its Jacobi update with mixing.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    int32_t L;                 /* momenta n = (nx*L + ny)*L + nz, n < L^3 */
+    int32_t n_blocks;          /* total momenta carried by hole pairs */
+    int32_t n_pmom, n_hmom;    /* particle / hole momenta (4 states each) */
+    int64_t n_t2;              /* blocked amplitudes = blk_off[n_blocks] */
+    int64_t n_m, n_w, n_rows;  /* m_off[n_blocks], w_off[n_blocks], row_off[n_blocks] */
+    int32_t n_tiles;           /* residual tiles (64 rows x 16 columns) */
+    int32_t pad0;
+    const int64_t *blk_off;    /* [n_blocks + 1] first amplitude of each block */
+    const int64_t *m_off;      /* [n_blocks + 1] M blocks [16][nc] */
+    const int64_t *w_off;      /* [n_blocks + 1] W blocks [nc][nc] */
+    const int64_t *row_off;    /* [n_blocks + 1] first row of each block (Y rows) */
+    const int32_t *blk_nr, *blk_nc, *blk_K;
+    const int32_t *blk_pm0, *blk_hm0; /* start of the block's lists in pm_list / hm_list */
+    const int32_t *pm_list;    /* particle-momentum index of each row group */
+    const int32_t *hm_list;    /* hole-momentum index of each column group */
+    const int32_t *ppos, *hpos; /* [n_blocks * L^3] row / column group of a momentum, or -1 */
+    const int32_t *kblk;       /* [L^3] block of a total momentum, or -1 */
+    const int32_t *pmom, *hmom; /* momentum of each particle / hole momentum index */
+    const int32_t *pinv, *hinv; /* [L^3] particle / hole momentum index, or -1 */
+    const int32_t *tiles;      /* [n_tiles * 3] (block, row0, col0) */
+    const double *V;           /* [256] V[s_p s_q s_r s_s] (antisymmetric pairs) */
+    const double *fpp;         /* [n_pmom * 16] Fock block of each particle momentum */
+    const double *fhh;         /* [n_hmom * 16] Fock block of each hole momentum */
+} nlb_pw_problem;
+
+typedef struct {
+    double *M;      /* [m_off[n]]   M_K[s_c s_d][col] = sum over k_c of t2 */
+    double *W;      /* [w_off[n]]   dressed hole-hole ladder */
+    double *Y;      /* [rows * 4]   row dots for X_pp */
+    double *Xpp;    /* [n_pmom * 16] */
+    double *Xhh;    /* [n_hmom * 16] */
+    double *R, *U, *G; /* [4 n_pmom * 4 n_hmom * 16] particle-hole intermediates */
+    double *H;      /* [n_t2] residual */
+    double *energy; /* [1] */
+} nlb_pw_state;
+
+/* MP2 start t2 = V / (e_i + e_j - e_a - e_b + delta) (coupled_cluster.py:416-439). */
+int nlb_pw_init(const nlb_pw_problem *P, double *t2, double delta, nlb_stream_t stream);
+/* M of t2 and E = 1/4 sum v_pphh t2 into S->energy (coupled_cluster.py:265-286). */
+int nlb_pw_energy(const nlb_pw_problem *P, const double *t2, nlb_pw_state *S, nlb_stream_t stream);
+/* One Jacobi step with mixing (S->M must hold M of t2): t2_out, and
+ * err = t2_out - t2 when err is not NULL. */
+int nlb_pw_step(const nlb_pw_problem *P, const double *t2, double *t2_out, double *err, double mixing,
+                nlb_pw_state *S, nlb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

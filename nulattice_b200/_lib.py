@@ -87,6 +87,19 @@ class ContractDesc(ctypes.Structure):
                                            "sa_k", "sb_k", "sa_b", "sb_b", "sc_b")]
 
 
+class PwProblem(ctypes.Structure):
+    _fields_ = [("L", c_int32), ("n_blocks", c_int32), ("n_pmom", c_int32), ("n_hmom", c_int32),
+                ("n_t2", c_int64), ("n_m", c_int64), ("n_w", c_int64), ("n_rows", c_int64),
+                ("n_tiles", c_int32), ("pad0", c_int32)] + \
+               [(n, c_void_p) for n in ("blk_off", "m_off", "w_off", "row_off", "blk_nr", "blk_nc", "blk_K",
+                                        "blk_pm0", "blk_hm0", "pm_list", "hm_list", "ppos", "hpos", "kblk",
+                                        "pmom", "hmom", "pinv", "hinv", "tiles", "V", "fpp", "fhh")]
+
+
+class PwState(ctypes.Structure):
+    _fields_ = [(n, c_void_p) for n in ("M", "W", "Y", "Xpp", "Xhh", "R", "U", "G", "H", "energy")]
+
+
 _lib = None
 _load_error = None
 
@@ -168,6 +181,12 @@ def lib():
     L.nlb_vec_diis_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]
     for name in ("nlb_contract_f64", "nlb_antisym_acc_f64", "nlb_ppph_intermediates_f64", "nlb_pppp_ladders_f64",
                  "nlb_jacobi_f64", "nlb_dense_energy_f64", "nlb_vec_diis_f64"):
+        getattr(L, name).restype = c_int32
+    L.nlb_pw_init.argtypes = [ctypes.POINTER(PwProblem), c_void_p, c_double, c_void_p]
+    L.nlb_pw_energy.argtypes = [ctypes.POINTER(PwProblem), c_void_p, ctypes.POINTER(PwState), c_void_p]
+    L.nlb_pw_step.argtypes = [ctypes.POINTER(PwProblem), c_void_p, c_void_p, c_void_p, c_double,
+                              ctypes.POINTER(PwState), c_void_p]
+    for name in ("nlb_pw_init", "nlb_pw_energy", "nlb_pw_step"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

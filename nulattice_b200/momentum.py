@@ -1,0 +1,322 @@
+"""Momentum-block CCSD for closed-shell plane-wave inputs.
+
+The plane-wave Hamiltonian of :mod:`nulattice_b200.planewave` (the lattice
+contact interaction in the momentum basis, normal-ordered with respect to
+closed momentum shells) is what the reference's ``ccsd_solver``
+(``CCM/coupled_cluster.py:547-687``) receives as dense blocks; the general
+engine then carries t2 as a dense p^2 h^2 tensor (4.4 GB at L=6, A=28) and
+evaluates ring terms of p^3 h^3 work.  This module solves the same equations
+in the structure those inputs have:
+
+* every hole momentum holds all four spin-isospin states, so f_ph = 0 and
+  every T1 term conserves momentum between a particle and a hole, which no
+  particle can: t1 stays zero and CCSD reduces to its T2 equation
+  (``coupled_cluster.py:476-536`` at t1 = 0);
+* t2[a,b,i,j] is non-zero only when k_a + k_b = k_i + k_j = K; it is stored
+  in one row-major block per total momentum K of a hole pair, rows
+  ``pa*16 + s_a*4 + s_b`` and columns ``pi*16 + s_i*4 + s_j``;
+* ``<pq||rs> = V[s_p s_q s_r s_s] delta(K)`` with V independent of the
+  momenta, so every diagram reduces to per-block sums and small
+  particle-hole intermediates (the kernels in ``csrc/momentum.cu``).
+
+The solver loop is the one of :func:`nulattice_b200.dense.solve` (MP2 start,
+Jacobi with mixing, the reference's convergence tests, pulsed DIIS of
+``CCM/soa/coupled_cluster.py:479-567``); its iterates equal the general
+engine's on the same inputs up to rounding.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import hamiltonian as _ham
+from . import planewave as _pw
+
+TILE_ROWS, TILE_COLS = 64, 16
+
+
+def _madd(L, k1, k2):
+    k1, k2 = np.asarray(k1), np.asarray(k2)
+    x = (k1 // (L * L) + k2 // (L * L)) % L
+    y = ((k1 // L) % L + (k2 // L) % L) % L
+    z = (k1 % L + k2 % L) % L
+    return (x * L + y) * L + z
+
+
+def _mneg(L, k):
+    k = np.asarray(k)
+    return ((-(k // (L * L)) % L) * L + (-((k // L) % L)) % L) * L + (-(k % L)) % L
+
+
+def contact_tensor(L, n_k, vT1, vS1, w3=0.0):
+    """``V[s_p s_q s_r s_s]`` (4^4) of the plane-wave two-body part: the
+    contact ``v_loc(vT1, vS1) / L^3`` plus the normal-ordered three-body part,
+    an SU(4) contact of strength ``2 n_k w3 / L^3`` (as in
+    :func:`planewave.plane_wave_hamiltonian`)."""
+    v = _pw._vloc_tensor(vT1, vS1) / L ** 3
+    if w3 != 0.0:
+        v3 = 2.0 * n_k * w3 / L ** 3
+        v = v + _pw._vloc_tensor(v3, v3) / L ** 3
+    return v
+
+
+def fock_blocks(L, n_k, hmom, pmom, vT1, vS1, w3=0.0):
+    """Per-momentum 4x4 Fock blocks and E_ref of
+    :func:`planewave.plane_wave_hamiltonian` in closed form: kinetic energy
+    on the diagonal, the hole trace ``n_k sum_s v2[s_a s s_c s]`` of the
+    two-body contact and the three-body ``f_3``; ``E_ref = tr f_hh - 1/2
+    sum <kl||kl> + E_3``."""
+    v2 = _pw._vloc_tensor(vT1, vS1) / L ** 3
+    tr2 = n_k * np.einsum("asbs->ab", v2)
+    if w3 != 0.0:
+        n_h = 4 * n_k
+        e3 = (n_h * (n_h - n_k) * (n_h - 2 * n_k)) / 6.0 * w3 / L ** 6
+        f3 = 0.5 * (3 * n_k) * (2 * n_k) * w3 / L ** 6
+    else:
+        e3 = f3 = 0.0
+
+    def kin(m):
+        m = np.asarray(m)
+        t = np.zeros(m.shape)
+        for c in (m // (L * L), (m // L) % L, m % L):
+            t += 2.0 - 2.0 * np.cos(2.0 * np.pi * c / L)
+        return t
+    eye = np.eye(4)
+    fpp = kin(pmom)[:, None, None] * eye + tr2[None] + f3 * eye
+    fhh = kin(hmom)[:, None, None] * eye + tr2[None] + f3 * eye
+    vt = contact_tensor(L, n_k, vT1, vS1, w3)
+    e_ref = float(np.trace(fhh, axis1=1, axis2=2).sum() - 0.5 * n_k ** 2 * np.einsum("stst->", vt) + e3)
+    return fpp, fhh, e_ref
+
+
+class MomentumPlan:
+    """Blocked layout of t2 for the closed shells ``holes`` on the L^3
+    lattice and the device tables of :c:type:`nlb_pw_problem`."""
+
+    def __init__(self, L, holes, device=None):
+        holes = np.asarray(holes, dtype=np.int64).reshape(-1, 5)
+        self.L = L = int(L)
+        n3 = L ** 3
+        self.hole, self.part = _ham.ph_split(holes, L)
+        hm_states = self.hole // 4
+        hmom = np.unique(hm_states)
+        if any(np.count_nonzero(hm_states == m) != 4 for m in hmom) or len(self.hole) != 4 * len(hmom):
+            raise ValueError("MomentumPlan: every hole momentum needs all four spin-isospin states")
+        self.hmom = hmom.astype(np.int64)
+        is_h = np.zeros(n3, bool); is_h[hmom] = True
+        self.pmom = np.nonzero(~is_h)[0].astype(np.int64)
+        self.n_k = len(hmom)
+        Ks = np.unique(_madd(L, hmom[:, None], hmom[None, :]).ravel())
+        self.Ks = Ks
+        pinv = -np.ones(n3, np.int32); pinv[self.pmom] = np.arange(len(self.pmom))
+        hinv = -np.ones(n3, np.int32); hinv[self.hmom] = np.arange(len(self.hmom))
+        kblk = -np.ones(n3, np.int32); kblk[Ks] = np.arange(len(Ks))
+        ppos = -np.ones((len(Ks), n3), np.int32)
+        hpos = -np.ones((len(Ks), n3), np.int32)
+        pm_list, hm_list, nr, nc, pm0, hm0 = [], [], [], [], [], []
+        for q, K in enumerate(Ks):
+            partner_p = _madd(L, K, _mneg(L, self.pmom))
+            pm = self.pmom[~is_h[partner_p]]
+            partner_h = _madd(L, K, _mneg(L, self.hmom))
+            hmk = self.hmom[is_h[partner_h]]
+            ppos[q, pm] = np.arange(len(pm)); hpos[q, hmk] = np.arange(len(hmk))
+            pm0.append(sum(len(x) for x in pm_list)); hm0.append(sum(len(x) for x in hm_list))
+            pm_list.append(pinv[pm]); hm_list.append(hinv[hmk])
+            nr.append(16 * len(pm)); nc.append(16 * len(hmk))
+        self.nr, self.nc = np.array(nr, np.int64), np.array(nc, np.int64)
+        self.blk_off = np.concatenate([[0], np.cumsum(self.nr * self.nc)]).astype(np.int64)
+        self.m_off = np.concatenate([[0], np.cumsum(16 * self.nc)]).astype(np.int64)
+        self.w_off = np.concatenate([[0], np.cumsum(self.nc * self.nc)]).astype(np.int64)
+        self.row_off = np.concatenate([[0], np.cumsum(self.nr)]).astype(np.int64)
+        self.n_t2 = int(self.blk_off[-1])
+        self.pm_list = np.concatenate(pm_list).astype(np.int32)
+        self.hm_list = np.concatenate(hm_list).astype(np.int32)
+        self.pm0, self.hm0 = np.array(pm0, np.int32), np.array(hm0, np.int32)
+        self.ppos, self.hpos, self.kblk, self.pinv, self.hinv = ppos, hpos, kblk, pinv, hinv
+        tiles = [(q, r0, c0) for q in range(len(Ks)) for r0 in range(0, int(self.nr[q]), TILE_ROWS)
+                 for c0 in range(0, int(self.nc[q]), TILE_COLS)]
+        self.tiles = np.array(tiles, np.int32).reshape(-1, 3)
+        self.p, self.h = len(self.part), len(self.hole)
+        self.dev = torch.device(device) if device is not None else None
+        self._dev_tables = None
+
+    # -- dense conversion (tests, small cases) ----------------------------
+    def _index_grid(self):
+        """Generic (a, b, i, j) of every blocked amplitude, in block order."""
+        L = self.L
+        pidx = -np.ones(4 * L ** 3, np.int64); pidx[self.part] = np.arange(self.p)
+        hidx = -np.ones(4 * L ** 3, np.int64); hidx[self.hole] = np.arange(self.h)
+        out = []
+        for q, K in enumerate(self.Ks):
+            pm = self.pmom[self.pm_list[self.pm0[q]:self.pm0[q] + self.nr[q] // 16]]
+            hm = self.hmom[self.hm_list[self.hm0[q]:self.hm0[q] + self.nc[q] // 16]]
+            ma = np.repeat(pm, 16); s = np.tile(np.arange(16), len(pm))
+            mb = _madd(L, K, _mneg(L, ma))
+            a = pidx[ma * 4 + s // 4]; b = pidx[mb * 4 + s % 4]
+            mi = np.repeat(hm, 16); u = np.tile(np.arange(16), len(hm))
+            mj = _madd(L, K, _mneg(L, mi))
+            i = hidx[mi * 4 + u // 4]; j = hidx[mj * 4 + u % 4]
+            out.append((np.repeat(a, len(i)), np.repeat(b, len(i)), np.tile(i, len(a)), np.tile(j, len(a))))
+        return tuple(np.concatenate([o[k] for o in out]) for k in range(4))
+
+    def to_dense(self, t2):
+        """Dense (p, p, h, h) array in the generic state order of
+        :func:`hamiltonian.ph_split` (small cases only)."""
+        t = np.asarray(t2.detach().cpu() if isinstance(t2, torch.Tensor) else t2, dtype=np.float64)
+        out = np.zeros((self.p, self.p, self.h, self.h))
+        out[self._index_grid()] = t
+        return out
+
+    def from_dense(self, t2):
+        """Blocked amplitudes of a dense (p, p, h, h) array."""
+        return np.asarray(t2, dtype=np.float64)[self._index_grid()]
+
+    # -- device problem ----------------------------------------------------
+    def problem(self, V, fpp, fhh, device):
+        """The :c:type:`nlb_pw_problem` with its tables on ``device``."""
+        dev = torch.device(device)
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
+        i64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=dev)  # noqa: E731
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
+        keep = dict(blk_off=i64(self.blk_off), m_off=i64(self.m_off), w_off=i64(self.w_off),
+                    row_off=i64(self.row_off), blk_nr=i32(self.nr), blk_nc=i32(self.nc), blk_K=i32(self.Ks),
+                    blk_pm0=i32(self.pm0), blk_hm0=i32(self.hm0), pm_list=i32(self.pm_list),
+                    hm_list=i32(self.hm_list), ppos=i32(self.ppos), hpos=i32(self.hpos), kblk=i32(self.kblk),
+                    pmom=i32(self.pmom), hmom=i32(self.hmom), pinv=i32(self.pinv), hinv=i32(self.hinv),
+                    tiles=i32(self.tiles), V=f64(np.asarray(V).reshape(256)), fpp=f64(np.asarray(fpp).reshape(-1)),
+                    fhh=f64(np.asarray(fhh).reshape(-1)))
+        P = _lib.PwProblem()
+        P.L, P.n_blocks, P.n_pmom, P.n_hmom = self.L, len(self.Ks), len(self.pmom), len(self.hmom)
+        P.n_t2, P.n_m, P.n_w, P.n_rows = self.n_t2, int(self.m_off[-1]), int(self.w_off[-1]), int(self.row_off[-1])
+        P.n_tiles = len(self.tiles)
+        for k, t in keep.items():
+            setattr(P, k, t.data_ptr())
+        return P, keep
+
+
+class MomentumEngine:
+    """Device tables, intermediates and the three entry points
+    (``nlb_pw_init`` / ``nlb_pw_energy`` / ``nlb_pw_step``) of one problem."""
+
+    def __init__(self, plan, V, fpp, fhh, device=None):
+        self.plan = plan
+        self.dev = torch.device(device if device is not None else "cuda")
+        self.L = _lib.lib()
+        self.P, self._keep = plan.problem(V, fpp, fhh, self.dev)
+        self.stream = torch.cuda.current_stream(self.dev)
+        self.sp = ctypes.c_void_p(self.stream.cuda_stream)
+        P = self.P
+        z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)  # noqa: E731
+        nph = 4 * P.n_pmom * 4 * P.n_hmom * 16
+        self.bufs = dict(M=z(P.n_m), W=z(P.n_w), Y=z(4 * P.n_rows), Xpp=z(16 * P.n_pmom), Xhh=z(16 * P.n_hmom),
+                         R=z(nph), U=z(nph), G=z(nph), H=z(plan.n_t2), energy=z(1))
+        self.S = _lib.PwState(**{k: v.data_ptr() for k, v in self.bufs.items()})
+        self.launches = 0
+
+    def zeros(self):
+        return torch.zeros(self.plan.n_t2, dtype=torch.float64, device=self.dev)
+
+    def init(self, t2, delta=0.0):
+        """MP2 start into ``t2``."""
+        _lib.check(self.L.nlb_pw_init(ctypes.byref(self.P), t2.data_ptr(), float(delta), self.sp), "pw init")
+        self.launches += 1
+
+    def energy(self, t2):
+        """Energy of ``t2`` (device scalar); also leaves M of ``t2`` for the next step."""
+        _lib.check(self.L.nlb_pw_energy(ctypes.byref(self.P), t2.data_ptr(), ctypes.byref(self.S), self.sp),
+                   "pw energy")
+        self.launches += 2
+        return self.bufs["energy"]
+
+    def step(self, t2, out, err=None, mixing=0.5):
+        """One Jacobi step with mixing from ``t2`` (M of ``t2`` current) into ``out``."""
+        _lib.check(self.L.nlb_pw_step(ctypes.byref(self.P), t2.data_ptr(), out.data_ptr(),
+                                      err.data_ptr() if err is not None else None, float(mixing),
+                                      ctypes.byref(self.S), self.sp), "pw step")
+        self.launches += 6
+
+
+def jacobi_gap(eng, t2):
+    """Largest change of one unmixed Jacobi step at ``t2``: zero at the CCSD
+    fixed point (the reference's residual test)."""
+    out = eng.zeros()
+    eng.energy(t2)
+    eng.step(t2, out, mixing=0.0)
+    return float((out - t2).abs().max().item())
+
+
+def solve(plan, V, fpp, fhh, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5, verbose=False,
+          criterion="soa", device=None, info=None, engine=None):
+    """The solver loop of :func:`nulattice_b200.dense.solve` on the blocked
+    amplitudes.  Returns ``(E_corr, t2)``, t2 blocked on the device."""
+    info = {} if info is None else info
+    t0 = time.perf_counter()
+    eng = engine if engine is not None else MomentumEngine(plan, V, fpp, fhh, device)
+    L, sp = eng.L, eng.sp
+    n = plan.n_t2
+    xs = [eng.zeros(), eng.zeros()]
+    cur = 0
+    eng.init(xs[0], delta)
+    use_diis = criterion == "soa" and max_diis > 0
+    if use_diis:
+        err = torch.zeros((max_diis, n), dtype=torch.float64, device=eng.dev)
+        hist = torch.zeros((max_diis, n), dtype=torch.float64, device=eng.dev)
+        work = torch.zeros(512, dtype=torch.float64, device=eng.dev)
+        nerr = 0
+    prev = float(eng.energy(xs[cur]).item())
+    if verbose:
+        print(f"Step 0: {prev}")
+    status, e, it = "max_iter", prev, 0
+    for it in range(1, maxSteps + 1):
+        eng.step(xs[cur], xs[cur ^ 1], err[nerr] if use_diis else None, mixing)
+        cur ^= 1
+        e = float(eng.energy(xs[cur]).item())
+        if verbose:
+            print(f"Step {it}: {e}", "difference =", abs(e - prev) / abs(e) if e != 0 else float("inf"))
+        if criterion == "soa":
+            done = abs(e - prev) / max(1.0, abs(e)) < eps
+        else:
+            done = (e == 0 and prev == 0) or (e != 0 and abs(e - prev) / abs(e) < eps)
+        if done:
+            status = "converged"
+            break
+        if use_diis:
+            hist[nerr].copy_(xs[cur])
+            nerr += 1
+            if nerr == max_diis:
+                _lib.check(L.nlb_vec_diis_f64(err.data_ptr(), hist.data_ptr(), n, max_diis, work.data_ptr(),
+                                              xs[cur].data_ptr(), sp), "pw diis")
+                eng.launches += 3
+                eng.energy(xs[cur])    # M of the extrapolated amplitudes for the next step
+                nerr = 0
+        if abs(e) > 1e10 or e != e:
+            status = "diverged"
+            break
+        prev = e
+    eng.stream.synchronize()
+    if status == "max_iter":
+        print("Max iterations reached.")
+    info.update(status=status, iterations=it, t_iterate=time.perf_counter() - t0, launches=eng.launches,
+                engine="momentum", n_t2=n, blocks=len(plan.Ks))
+    return e, xs[cur]
+
+
+def ccsd_plane_wave(L, holes, vT1, vS1, w3=0.0, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5,
+                    verbose=False, criterion="soa", device=None, info=None):
+    """CCSD of the closed-shell plane-wave Hamiltonian
+    :func:`planewave.plane_wave_hamiltonian` ``(L, holes, vT1, vS1, w3)`` on
+    the momentum blocks.  Returns ``(E_corr, E_ref, t2, plan)``: t2 blocked
+    on the device (``plan.to_dense`` gives the reference's layout)."""
+    info = {} if info is None else info
+    t0 = time.perf_counter()
+    plan = MomentumPlan(L, holes)
+    V = contact_tensor(L, plan.n_k, vT1, vS1, w3)
+    fpp, fhh, e_ref = fock_blocks(L, plan.n_k, plan.hmom, plan.pmom, vT1, vS1, w3)
+    info["t_plan"] = time.perf_counter() - t0
+    e, t2 = solve(plan, V, fpp, fhh, eps=eps, maxSteps=maxSteps, max_diis=max_diis, delta=delta, mixing=mixing,
+                  verbose=verbose, criterion=criterion, device=device, info=info)
+    return e, e_ref, t2, plan
