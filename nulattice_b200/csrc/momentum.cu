@@ -162,6 +162,9 @@ __global__ void k_pw_energy(nlb_pw_problem P, const double* __restrict__ M, doub
 // One warp per row (pa, s_b, s_d) of every block:
 //   Y[row][s_c] = sum_c V[s_c s_d][spins of c] T[row][c]
 __global__ void k_pw_xrow(nlb_pw_problem P, const double* __restrict__ t2, double* __restrict__ Y) {
+    __shared__ double Vs[256];
+    for (int q = threadIdx.x; q < 256; q += blockDim.x) Vs[q] = P.V[q];
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t nrows = P.n_rows;
     const int64_t wpb = blockDim.x >> 5;
@@ -175,10 +178,10 @@ __global__ void k_pw_xrow(nlb_pw_problem P, const double* __restrict__ t2, doubl
         for (int c = lane; c < nc; c += 32) {
             const double x = T[c];
             const int sp = c & 15;
-            a0 += P.V[(0 * 4 + sd) * 16 + sp] * x;
-            a1 += P.V[(1 * 4 + sd) * 16 + sp] * x;
-            a2 += P.V[(2 * 4 + sd) * 16 + sp] * x;
-            a3 += P.V[(3 * 4 + sd) * 16 + sp] * x;
+            a0 += Vs[(0 * 4 + sd) * 16 + sp] * x;
+            a1 += Vs[(1 * 4 + sd) * 16 + sp] * x;
+            a2 += Vs[(2 * 4 + sd) * 16 + sp] * x;
+            a3 += Vs[(3 * 4 + sd) * 16 + sp] * x;
         }
         for (int o = 16; o > 0; o >>= 1) {
             a0 += __shfl_xor_sync(0xffffffffu, a0, o);
@@ -259,6 +262,9 @@ __global__ void k_pw_W(nlb_pw_problem P, const double* __restrict__ M, double* _
 //   U[s_d s_l] = sum V[s_c s_d s_k s_l] R[s_c s_k]          (dgram_cdkl_acik_dblj, ccDgrams.py:279-290)
 __global__ void k_pw_R(nlb_pw_problem P, const double* __restrict__ t2, double* __restrict__ R,
                        double* __restrict__ U, double* __restrict__ G) {
+    __shared__ double Vs[256];
+    for (int q = threadIdx.x; q < 256; q += blockDim.x) Vs[q] = P.V[q];
+    __syncthreads();
     const int L = P.L, L3 = L * L * L;
     const int nps = 4 * P.n_pmom, nhs = 4 * P.n_hmom;
     const int64_t n = (int64_t)nps * nhs;
@@ -295,8 +301,8 @@ __global__ void k_pw_R(nlb_pw_problem P, const double* __restrict__ t2, double* 
                 for (int sc = 0; sc < 4; ++sc)
 #pragma unroll
                     for (int sk = 0; sk < 4; ++sk) {
-                        g += P.V[((x * 4 + sk) * 4 + sc) * 4 + y] * r[sc * 4 + sk];
-                        u += P.V[((sc * 4 + x) * 4 + sk) * 4 + y] * r[sc * 4 + sk];
+                        g += Vs[((x * 4 + sk) * 4 + sc) * 4 + y] * r[sc * 4 + sk];
+                        u += Vs[((sc * 4 + x) * 4 + sk) * 4 + y] * r[sc * 4 + sk];
                     }
                 Go[x * 4 + y] = -g;
                 Uo[x * 4 + y] = u;
@@ -317,8 +323,13 @@ __device__ __forceinline__ double dot16(const double* __restrict__ x, const doub
 }
 
 // ------------------------------------------------------------- residual ----
-// One CTA per tile of 64 rows x 16 columns of one block: T_K W_K for the tile
-// through shared memory, then every other term of the residual per amplitude.
+// One CTA per tile of 64 rows (four whole row groups pa) x 16 columns (one
+// column group pi) of one block: T_K W_K for the tile through shared memory,
+// then every other term of the residual per amplitude.  The tile's own T
+// values (all the X_pp / X_hh terms need), V and the momenta of the tile's
+// row and column groups sit in shared memory.  The quadratic ring term uses
+// Z(ai, bj) = R_ai V R_bj = Z(bj, ai) (V[c d k l] = V[d c l k]), so its four
+// images reduce to 2 (Z(ai, bj) - Z(bi, aj)).
 constexpr int kTR = 64, kTC = 16;
 
 __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const double* __restrict__ t2,
@@ -327,13 +338,33 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
                                                      const double* __restrict__ R, const double* __restrict__ U,
                                                      const double* __restrict__ G, double* __restrict__ H) {
     __shared__ double Ts[kTR][kTC + 1];
+    __shared__ double Town[kTR][kTC + 1];
     __shared__ double Ws[kTC][kTC + 1];
+    __shared__ double Vs[256];
+    __shared__ int s_ma[4], s_mb[4], s_mi, s_mj;
     const int tid = threadIdx.x;
     const int cc = tid & 15, rr = tid >> 4;
     const int nhs = 4 * P.n_hmom;
+    const int L = P.L;
+    Vs[tid] = P.V[tid];
     for (int tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
         const int b = P.tiles[3 * tile], r0 = P.tiles[3 * tile + 1], c0 = P.tiles[3 * tile + 2];
-        const int nr = P.blk_nr[b], nc = P.blk_nc[b];
+        const int nr = P.blk_nr[b], nc = P.blk_nc[b], K = P.blk_K[b];
+        __syncthreads();   // the previous tile's epilogue is done with the shared tables
+        if (tid < 4) {
+            const int pa = (r0 >> 4) + tid;
+            int ma = 0, mb = 0;
+            if (pa * 16 < nr) {
+                ma = P.pm_list[P.blk_pm0[b] + pa];
+                mb = P.pinv[msub(K, P.pmom[ma], L)];
+            }
+            s_ma[tid] = ma;
+            s_mb[tid] = mb;
+        } else if (tid == 4) {
+            const int mi = P.hm_list[P.blk_hm0[b] + (c0 >> 4)];
+            s_mi = mi;
+            s_mj = P.hinv[msub(K, P.hmom[mi], L)];
+        }
         const double* T = t2 + P.blk_off[b];
         const double* Wb = W + P.w_off[b];
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -344,7 +375,9 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
                 const int e = tid + 256 * q;
                 const int rrow = e >> 4, kk = e & 15;
                 const int r = r0 + rrow;
-                Ts[rrow][kk] = (r < nr) ? T[(int64_t)r * nc + k0 + kk] : 0.0;
+                const double x = (r < nr) ? T[(int64_t)r * nc + k0 + kk] : 0.0;
+                Ts[rrow][kk] = x;
+                if (k0 == c0) Town[rrow][kk] = x;
             }
             Ws[rr][cc] = Wb[(int64_t)(k0 + rr) * nc + c0 + cc];
             __syncthreads();
@@ -356,44 +389,48 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
             }
         }
         const double* Mb = M + P.m_off[b];
+        const int c = c0 + cc;
+        const int si = (cc >> 2) & 3, sj = cc & 3, sa = (rr >> 2) & 3, sb = rr & 3;
+        const int sab = sa * 4 + sb, sij = si * 4 + sj;
+        const int mi = s_mi, mj = s_mj;
+        // 1/2 v_pppp t2 through M: the same 16 M values for the four rows
+        double lad = 0.0;
+#pragma unroll
+        for (int sg = 0; sg < 16; ++sg) lad += Vs[sab * 16 + sg] * Mb[(int64_t)sg * nc + c];
+        double xhh_j[4], xhh_i[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            xhh_j[s] = Xhh[mj * 16 + s * 4 + sj];
+            xhh_i[s] = Xhh[mi * 16 + s * 4 + si];
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int r = r0 + rr + 16 * q;
+            const int rl = rr + 16 * q;
+            const int r = r0 + rl;
             if (r >= nr) continue;
-            const Amp A = decode_amp(P, b, r, c0 + cc);
-            const int c = A.c;
-            const int sab = A.sa * 4 + A.sb, sij = A.si * 4 + A.sj;
-            // v_pphh, and 1/2 v_pppp t2 through M (ccDgrams.py:215-237)
-            double h = P.V[sab * 16 + sij];
-            double lad = 0.0;
-#pragma unroll 4
-            for (int sg = 0; sg < 16; ++sg) lad += P.V[sab * 16 + sg] * Mb[(int64_t)sg * nc + c];
-            h += 0.5 * lad;
-            // hole-hole ladders
-            h += acc[q];
+            const int ma = s_ma[q], mb = s_mb[q];
+            // v_pphh, 1/2 v_pppp t2 (ccDgrams.py:215-237), hole-hole ladders
+            double h = Vs[sab * 16 + sij] + 0.5 * lad + acc[q];
             // P(ab) X_pp t2 and P(ij) X_hh t2 (coupled_cluster.py:536)
-            const int pa = r >> 4, pi = c >> 4;
-            const double* Tr = T + (int64_t)r * nc;
             double xp = 0.0, xh = 0.0;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-                xp += Xpp[A.mb * 16 + A.sb * 4 + s] * T[(int64_t)(pa * 16 + A.sa * 4 + s) * nc + c];
-                xp += Xpp[A.ma * 16 + A.sa * 4 + s] * T[(int64_t)(pa * 16 + s * 4 + A.sb) * nc + c];
-                xh += Xhh[A.mj * 16 + s * 4 + A.sj] * Tr[pi * 16 + A.si * 4 + s];
-                xh += Xhh[A.mi * 16 + s * 4 + A.si] * Tr[pi * 16 + s * 4 + A.sj];
+                xp += Xpp[mb * 16 + sb * 4 + s] * Town[q * 16 + sa * 4 + s][cc];
+                xp += Xpp[ma * 16 + sa * 4 + s] * Town[q * 16 + s * 4 + sb][cc];
+                xh += xhh_j[s] * Town[rl][si * 4 + s];
+                xh += xhh_i[s] * Town[rl][s * 4 + sj];
             }
             h += xp + xh;
-            // rings and the quadratic ring term over the four images
-            const int64_t a = A.ma * 4 + A.sa, bb = A.mb * 4 + A.sb;
-            const int64_t i = A.mi * 4 + A.si, j = A.mj * 4 + A.sj;
+            // rings (four images of G) and the quadratic ring term
+            const int64_t a = ma * 4 + sa, bb = mb * 4 + sb;
+            const int64_t i = mi * 4 + si, j = mj * 4 + sj;
             const int64_t ai = (a * nhs + i) * 16, bi = (bb * nhs + i) * 16;
             const int64_t aj = (a * nhs + j) * 16, bj = (bb * nhs + j) * 16;
-            const double ring = ((G[ai + A.sb * 4 + A.sj] - G[bi + A.sa * 4 + A.sj]) -
-                                 (G[aj + A.sb * 4 + A.si] - G[bj + A.sa * 4 + A.si]));
-            const double quad = ((dot16(U + ai, R + bj) - dot16(U + bi, R + aj)) -
-                                 (dot16(U + aj, R + bi) - dot16(U + bj, R + ai)));
-            h += ring + 0.5 * quad;
-            H[A.off + (int64_t)r * nc + c] = h;
+            const double ring = ((G[ai + sb * 4 + sj] - G[bi + sa * 4 + sj]) -
+                                 (G[aj + sb * 4 + si] - G[bj + sa * 4 + si]));
+            const double quad = dot16(U + ai, R + bj) - dot16(U + bi, R + aj);
+            h += ring + quad;
+            H[P.blk_off[b] + (int64_t)r * nc + c] = h;
         }
     }
 }
