@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the dE/dC2, dE/dC3 leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batched scan")
     ap.add_argument("--profile-lambda", action="store_true", help="one short Lambda solve at L=6, A=28 (for ncu)")
+    ap.add_argument("--profile-planewave", action="store_true",
+                    help="momentum-block solves of closed-shell plane waves (L=6 A=4, L=6 A=28, L=8 A=28), "
+                         "and 20 timed steps of each; no JSON")
     return ap.parse_args()
 
 
@@ -185,6 +188,40 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def profile_planewave(dev):
+    """Momentum-block path on closed-shell plane waves (couplings vT1 = vS1 =
+    -4, w3 = 1): two solves to 1e-10 (pulsed DIIS 8) on a warm engine, wall
+    clock, then 20 steps timed with CUDA events."""
+    import torch
+    from nulattice_b200 import momentum as MB
+    from nulattice_b200 import planewave as PW
+    for (L, A) in ((6, 4), (6, 28), (8, 28)):
+        plan = MB.MomentumPlan(L, PW.momentum_holes(L, A))
+        V = MB.contact_tensor(L, plan.n_k, -4.0, -4.0, 1.0)
+        fpp, fhh, e_ref = MB.fock_blocks(L, plan.n_k, plan.hmom, plan.pmom, -4.0, -4.0, 1.0)
+        eng = MB.MomentumEngine(plan, V, fpp, fhh, dev)
+        for _ in range(2):
+            info = {}
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            e, t2 = MB.solve(plan, V, fpp, fhh, eps=1e-10, maxSteps=1000, max_diis=8, engine=eng, info=info)
+            torch.cuda.synchronize(dev)
+            print(f"L={L} A={A} n_t2={plan.n_t2} E_corr={e:.12f} {info['status']} iterations={info['iterations']} "
+                  f"solve_s={time.perf_counter() - t0:.4f}", flush=True)
+        x, y = eng.zeros(), eng.zeros()
+        eng.init(x)
+        eng.energy(x)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for _ in range(3):
+            eng.step(x, y)
+        ev[0].record()
+        for _ in range(20):
+            eng.step(x, y)
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        print(f"   step_us={ev[0].elapsed_time(ev[1]) / 20 * 1e3:.1f}", flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -197,6 +234,9 @@ def main():
     from nulattice_b200 import hamiltonian as ham
     from nulattice_b200 import structure as S
 
+    if args.profile_planewave:
+        profile_planewave(torch.device("cuda", 0))
+        return
     rank, ws, local = dist_setup()
     dev = torch.device("cuda", local)
     e_ref, fock, two = build_problem(L_BENCH, A_BENCH)
