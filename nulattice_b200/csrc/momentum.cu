@@ -126,10 +126,12 @@ __global__ void k_pw_init(nlb_pw_problem P, double* t2, double delta) {
 }
 
 // ------------------------------------------------------------ M, energy ----
-// M_K[sigma][c] = sum_pa T_K[pa*16 + sigma][c]
+// M_K[sigma][c] = sum_pa T_K[pa*16 + sigma][c]: one warp per entry, the
+// lanes over the row groups pa, summed by a fixed shuffle tree.
 __global__ void k_pw_M(nlb_pw_problem P, const double* __restrict__ t2, double* __restrict__ M) {
-    const int64_t n = P.n_m;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wpb = blockDim.x >> 5;
+    for (int64_t e = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); e < P.n_m; e += (int64_t)gridDim.x * wpb) {
         const int b = seg_of(P.m_off, P.n_blocks, e);
         const int nc = P.blk_nc[b];
         const int64_t loc = e - P.m_off[b];
@@ -137,8 +139,9 @@ __global__ void k_pw_M(nlb_pw_problem P, const double* __restrict__ t2, double* 
         const int npa = P.blk_nr[b] >> 4;
         const double* T = t2 + P.blk_off[b] + (int64_t)sg * nc + c;
         double acc = 0.0;
-        for (int pa = 0; pa < npa; ++pa) acc += T[(int64_t)pa * 16 * nc];
-        M[e] = acc;
+        for (int pa = lane; pa < npa; pa += 32) acc += T[(int64_t)pa * 16 * nc];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) M[e] = acc;
     }
 }
 
@@ -485,7 +488,7 @@ int nlb_pw_init(const nlb_pw_problem* P, double* t2, double delta, nlb_stream_t 
 int nlb_pw_energy(const nlb_pw_problem* P, const double* t2, nlb_pw_state* S, nlb_stream_t stream) {
     if (!pw_ok(P) || !t2 || !S || !S->M || !S->energy) return pfail(NLB_ERR_ARG, "nlb_pw_energy: bad argument");
     cudaStream_t st = (cudaStream_t)stream;
-    k_pw_M<<<pgrid(P->n_m), 256, 0, st>>>(*P, t2, S->M);
+    k_pw_M<<<pgrid(32 * P->n_m), 256, 0, st>>>(*P, t2, S->M);
     k_pw_energy<<<1, 256, 0, st>>>(*P, S->M, S->energy);
     return pcheck("nlb_pw_energy");
 }
