@@ -81,3 +81,32 @@ def test_contact_tensor_is_antisymmetric_and_the_builder_value():
     v3 = 2.0 * nk * 0.7 / L ** 3
     np.testing.assert_allclose(v, (PW._vloc_tensor(-6.0, -5.0) + PW._vloc_tensor(v3, v3)) / L ** 3, rtol=1e-15)
     assert ham.contact_couplings(-3.0, 1.0) == (-6.0, 2.0)
+
+
+@pytest.mark.parametrize("L,A,w3", [(3, 4, 0.7), (3, 28, 0.7)])
+def test_blocked_residual_model_matches_the_oracle(L, A, w3):
+    """The blocked algebra of the momentum-block kernels (CPU model in
+    momentum_model.py) against the oracle's dense T2 residual and dressed
+    Fock blocks, at random antisymmetric momentum-conserving amplitudes."""
+    import momentum_model as MM
+    from oracle import ccsd_oracle as O
+    holes = PW.momentum_holes(L, A)
+    e_ref, fock, two = PW.plane_wave_hamiltonian(L, holes, -6.0, -5.0, w3, dense=True)
+    plan = MB.MomentumPlan(L, holes)
+    V = MB.contact_tensor(L, plan.n_k, -6.0, -5.0, w3)
+    fpp, fhh, _ = MB.fock_blocks(L, plan.n_k, plan.hmom, plan.pmom, -6.0, -5.0, w3)
+    t2 = plan.to_dense(np.random.default_rng(3).standard_normal(plan.n_t2) * 1e-2)
+    t2 = 0.25 * ((t2 - t2.transpose(1, 0, 2, 3)) - (t2.transpose(0, 1, 3, 2) - t2.transpose(1, 0, 3, 2)))
+    H, Xpp, Xhh = MM.residual(plan, V, fpp, fhh, plan.from_dense(t2))
+    h2o, xppo, xhho = O.t2_residual(O.Hamiltonian(fock, two), np.zeros((plan.p, plan.h)), t2)
+    # the oracle's residual vanishes outside the momentum blocks
+    assert np.abs(h2o).sum() == pytest.approx(np.abs(plan.from_dense(h2o)).sum(), rel=1e-14)
+    np.testing.assert_allclose(H, plan.from_dense(h2o), rtol=0, atol=1e-13 * np.abs(h2o).max())
+    pidx = {int(x): q for q, x in enumerate(plan.part)}
+    hidx = {int(x): q for q, x in enumerate(plan.hole)}
+    for q, m in enumerate(plan.pmom):
+        ix = [pidx[int(m) * 4 + s] for s in range(4)]
+        np.testing.assert_allclose(Xpp[q], xppo[np.ix_(ix, ix)], rtol=0, atol=1e-13)
+    for q, m in enumerate(plan.hmom):
+        ix = [hidx[int(m) * 4 + s] for s in range(4)]
+        np.testing.assert_allclose(Xhh[q], xhho[np.ix_(ix, ix)], rtol=0, atol=1e-13)
