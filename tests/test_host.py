@@ -200,3 +200,39 @@ def test_dense_blocks_are_row_major_whatever_the_input_strides():
         assert t.is_contiguous() and t.dtype.is_floating_point
         np.testing.assert_array_equal(t.numpy(), y)
         assert Dn._dense_block(torch.as_tensor(y), None, "cpu").is_contiguous()
+
+
+PAIRS = [("StructProblem", "nlb_struct_problem"), ("Ctrl", "nlb_ctrl"), ("StructState", "nlb_struct_state"),
+         ("LambdaState", "nlb_lambda_state"), ("BatchItem", "nlb_batch_item"), ("BatchConfig", "nlb_batch_config"),
+         ("ContractDesc", "nlb_contract_desc"), ("PwProblem", "nlb_pw_problem"), ("PwState", "nlb_pw_state")]
+
+
+def test_ctypes_mirrors_match_the_c_header(tmp_path):
+    """Every ctypes mirror in _lib has the size and the field offsets that a
+    C compiler gives the struct of include/nulattice_b200.h."""
+    import os
+    import shutil
+    import subprocess
+    from nulattice_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "nulattice_b200.h"', "int main(void) {"]
+    want = []
+    for py, c in PAIRS:
+        cls = getattr(_lib, py)
+        lines.append(f'printf("%zu\\n", sizeof({c}));')
+        want.append((py, "sizeof", ctypes.sizeof(cls)))
+        for name, _ in cls._fields_:
+            lines.append(f'printf("%zu\\n", offsetof({c}, {name}));')
+            want.append((py, name, getattr(cls, name).offset))
+    lines += ["return 0;", "}"]
+    src = tmp_path / "abi.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "abi"
+    subprocess.run([cc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert len(got) == len(want)
+    bad = [(w, g) for w, g in zip(want, got) if w[2] != g]
+    assert not bad, bad
