@@ -97,7 +97,7 @@ class MomentumPlan:
     """Blocked layout of t2 for the closed shells ``holes`` on the L^3
     lattice and the device tables of :c:type:`nlb_pw_problem`."""
 
-    def __init__(self, L, holes, device=None):
+    def __init__(self, L, holes):
         holes = np.asarray(holes, dtype=np.int64).reshape(-1, 5)
         self.L = L = int(L)
         n3 = L ** 3
@@ -141,8 +141,6 @@ class MomentumPlan:
                  for c0 in range(0, int(self.nc[q]), TILE_COLS)]
         self.tiles = np.array(tiles, np.int32).reshape(-1, 3)
         self.p, self.h = len(self.part), len(self.hole)
-        self.dev = torch.device(device) if device is not None else None
-        self._dev_tables = None
 
     # -- dense conversion (tests, small cases) ----------------------------
     def _index_grid(self):
