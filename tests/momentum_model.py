@@ -90,3 +90,20 @@ def residual(plan, V, fpp, fhh, t):
         HK = HK + (xp + xh + ring + quad).reshape(nr, nc)
         H[plan.blk_off[q]:plan.blk_off[q + 1]] = HK.ravel()
     return H, Xpp, Xhh
+
+
+def step(plan, V, fpp, fhh, t, mixing=0.5):
+    """One Jacobi step with mixing on the blocked amplitudes: the residual,
+    the denominators -(X_pp[a,a] + X_pp[b,b] + X_hh[i,i] + X_hh[j,j]) from
+    the diagonals of the 4x4 blocks, ``m t + (1 - m)(t + H / D)``."""
+    t = np.asarray(t, dtype=np.float64)
+    H, Xpp, Xhh = residual(plan, V, fpp, fhh, t)
+    dp, dh = np.einsum("mss->ms", Xpp), np.einsum("mss->ms", Xhh)
+    D = np.zeros(plan.n_t2)
+    for q in range(len(plan.Ks)):
+        ma, mb, mi, mj = _group_momenta(plan, q)
+        npa, nhg = len(ma), len(mi)
+        drow = (dp[ma][:, :, None] + dp[mb][:, None, :]).reshape(npa * 16)     # [pa, sa, sb]
+        dcol = (dh[mi][:, :, None] + dh[mj][:, None, :]).reshape(nhg * 16)     # [pi, si, sj]
+        D[plan.blk_off[q]:plan.blk_off[q + 1]] = (-(drow[:, None] + dcol[None, :])).ravel()
+    return mixing * t + (1.0 - mixing) * (t + H / D)

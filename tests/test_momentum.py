@@ -110,3 +110,21 @@ def test_blocked_residual_model_matches_the_oracle(L, A, w3):
     for q, m in enumerate(plan.hmom):
         ix = [hidx[int(m) * 4 + s] for s in range(4)]
         np.testing.assert_allclose(Xhh[q], xhho[np.ix_(ix, ix)], rtol=0, atol=1e-13)
+
+
+def test_blocked_jacobi_step_model_matches_the_oracle():
+    """One mixed Jacobi step of the blocked model from the MP2 start against
+    the oracle's solver loop (one step, no DIIS) on the dense blocks."""
+    import momentum_model as MM
+    from oracle import ccsd_oracle as O
+    L, A, w3 = 3, 4, 0.7
+    holes = PW.momentum_holes(L, A)
+    e_ref, fock, two = PW.plane_wave_hamiltonian(L, holes, -6.0, -5.0, w3, dense=True)
+    plan = MB.MomentumPlan(L, holes)
+    V = MB.contact_tensor(L, plan.n_k, -6.0, -5.0, w3)
+    fpp, fhh, _ = MB.fock_blocks(L, plan.n_k, plan.hmom, plan.pmom, -6.0, -5.0, w3)
+    _, _, t0, _, _ = O.solve(fock, two, eps=0.0, maxSteps=0, max_diis=0, criterion="numpy")
+    _, t1o, t2o, _, _ = O.solve(fock, two, eps=0.0, maxSteps=1, max_diis=0, criterion="numpy")
+    assert not np.any(t1o)
+    t1 = MM.step(plan, V, fpp, fhh, plan.from_dense(t0), 0.5)
+    np.testing.assert_allclose(t1, plan.from_dense(t2o), rtol=0, atol=1e-13 * np.abs(t2o).max())
