@@ -128,3 +128,18 @@ def test_blocked_jacobi_step_model_matches_the_oracle():
     assert not np.any(t1o)
     t1 = MM.step(plan, V, fpp, fhh, plan.from_dense(t0), 0.5)
     np.testing.assert_allclose(t1, plan.from_dense(t2o), rtol=0, atol=1e-13 * np.abs(t2o).max())
+
+
+def test_c_abi_rejects_incomplete_problems_before_any_launch():
+    """The momentum-block entry points check their descriptors on the host
+    and return NLB_ERR_ARG with a message (no CUDA call is made)."""
+    import ctypes
+    from nulattice_b200 import _lib
+    L = _lib.lib()
+    P, S = _lib.PwProblem(), _lib.PwState()
+    assert L.nlb_pw_init(None, None, 0.0, None) == _lib.NLB_ERR_ARG
+    assert b"nlb_pw_init" in L.nlb_last_error()
+    assert L.nlb_pw_energy(ctypes.byref(P), None, ctypes.byref(S), None) == _lib.NLB_ERR_ARG
+    assert b"nlb_pw_energy" in L.nlb_last_error()
+    assert L.nlb_pw_step(ctypes.byref(P), None, None, None, 0.5, ctypes.byref(S), None) == _lib.NLB_ERR_ARG
+    assert b"nlb_pw_step" in L.nlb_last_error()
