@@ -138,8 +138,11 @@ int nlb_version(void);
 const char *nlb_last_error(void);
 
 /* Length (doubles) of the dressed-Fock scratch: Q, X_hh (T2 eq), X_hh (T1 eq)
- * as h*h each, the particle diagonals of X_pp for both equations, and the
- * per-label compact tables t1[P_g,H_g], X_hh[H_g,H_g], diag X_pp, diag X_hh. */
+ * as h*h each, the particle diagonals of X_pp for both equations, the
+ * per-label compact tables t1[P_g,H_g], X_hh[H_g,H_g], diag X_pp, diag X_hh,
+ * and the per-block partial sums of the step's reductions (energy, norms,
+ * DIIS Gram matrix), which the consuming kernel adds in a fixed order so that
+ * every solve repeats bit for bit. */
 int64_t nlb_struct_prep_len(const nlb_struct_problem *prob);
 
 /* Dynamic shared memory (bytes) the T2-update kernel needs per block for
@@ -175,11 +178,14 @@ int nlb_struct_stage(const nlb_struct_problem *prob, const nlb_struct_state *st,
  * usual; st->g, st->f2 and st->prep are ignored.  The step's scratch comes
  * from a fixed 8 MiB array in device memory that every GPU loading this
  * library holds until exit; a problem that needs more (see
- * nlb_struct_noalloc_scratch_bytes) is rejected with NLB_ERR_SIZE.  The first
- * call on a device looks up the array's device address, so make it before
- * any stream capture.  All calls share the array: calls that overlap on the
- * GPU (other streams, other threads) race and must not be issued.  Nothing is
- * allocated or freed. */
+ * nlb_struct_noalloc_scratch_bytes) is rejected with NLB_ERR_SIZE, and so is
+ * a problem with negative sizes.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other
+ * threads) race and must not be issued.  Nothing is allocated or freed.
+ * The step fills the DIIS rings when they are given; the extrapolation
+ * (nlb_struct_diis) needs st->prep for its partial sums, while
+ * nlb_struct_energy needs no scratch. */
 int nlb_struct_step_noalloc(const nlb_struct_problem *prob, const nlb_struct_state *st,
                             nlb_stream_t stream);
 /* Bytes of the static scratch nlb_struct_step_noalloc needs for this problem
@@ -190,12 +196,15 @@ int64_t nlb_struct_noalloc_scratch_bytes(const nlb_struct_problem *prob, int32_t
  * ctrl->diis_pulse is set, build the Gram matrix of the stored error vectors
  * (FP64), solve the bordered system in FP64 on the device and extrapolate the
  * current amplitudes in place.  No-op otherwise.  `max_diis` must equal the
- * value given to nlb_struct_ctrl_init (it selects the compiled kernel). */
+ * value given to nlb_struct_ctrl_init (it selects the compiled kernel).
+ * Reads t1, t2, the rings, ctrl and the partial-sum area of st->prep; st->g
+ * and st->f2 are not used. */
 int nlb_struct_diis(const nlb_struct_problem *prob, const nlb_struct_state *st, int32_t max_diis,
                     nlb_stream_t stream);
 
 /* Energy of the current amplitudes, sum_ai f_ai t1_ai (ccsd_energy,
- * coupled_cluster.py:265-286, with v_pphh = 0), written to *e_out (device). */
+ * coupled_cluster.py:265-286, with v_pphh = 0), written to *e_out (device).
+ * Reads t1, f_ph and ctrl only (no scratch). */
 int nlb_struct_energy(const nlb_struct_problem *prob, const nlb_struct_state *st,
                       double *e_out, nlb_stream_t stream);
 
@@ -340,16 +349,40 @@ int nlb_antisym_acc_f64(const double *Z, double *H, int64_t p, int64_t h, int32_
  * antisymmetry in floating point; identity on exactly antisymmetric H. */
 int nlb_antisym_project_f64(double *H, int64_t p, int64_t h, nlb_stream_t stream);
 
-/* v_ppph_dgrams (ccDgrams.py:13-45): r[0..6] zero-filled by the caller, rows
- * idx[q] = (c,d,a,k) with value val[q]; repeated keys add up. */
-int nlb_ppph_intermediates_f64(const int64_t *idx, const double *val, int64_t nnz, const double *t1,
-                               const double *t2, int64_t p, int64_t h, double *const *r,
-                               nlb_stream_t stream);
+/* Row list of v_ppph, idx[q] = (c,d,a,k) with value val[q] (repeated keys
+ * add up), with the orders its intermediates are gathered in.  perm_* list
+ * the rows sorted by the named key (a stable sort, so rows with equal keys
+ * keep their list order); seg_*[s] .. seg_*[s+1] is the range of key s in that
+ * order (n_* keys, seg_* has n_* + 1 entries).  perm_adk sorts by (a, d, k),
+ * and seg_a, seg_ad and seg_adk all index it.  Built once per problem on the
+ * host; every output entry is then the sum of its rows in a fixed order. */
+typedef struct {
+    int64_t nnz;
+    const int64_t *idx;          /* [nnz][4] (c, d, a, k) */
+    const double *val;           /* [nnz] */
+    const int32_t *perm_adk, *perm_ak, *perm_cdk;
+    int64_t n_a, n_ad, n_adk, n_ak, n_cdk;
+    const int64_t *seg_a, *seg_ad, *seg_adk, *seg_ak, *seg_cdk;
+} nlb_ppph_plan;
+
+/* Row list of v_pppp, idx[q] = (a,b,c,d), sorted by (a, b) through perm_ab
+ * with the n_ab key ranges seg_ab (as above). */
+typedef struct {
+    int64_t nnz;
+    const int64_t *idx;
+    const double *val;
+    const int32_t *perm_ab;
+    int64_t n_ab;
+    const int64_t *seg_ab;
+} nlb_pppp_plan;
+
+/* v_ppph_dgrams (ccDgrams.py:13-45): r[0..6] zero-filled by the caller. */
+int nlb_ppph_intermediates_f64(const nlb_ppph_plan *plan, const double *t1, const double *t2, int64_t p,
+                               int64_t h, double *const *r, nlb_stream_t stream);
 
 /* v_pppp_dgrams (ccDgrams.py:215-237): l1 += v t2[c,d], l2 += v t1[c] t1[d]. */
-int nlb_pppp_ladders_f64(const int64_t *idx, const double *val, int64_t nnz, const double *t1,
-                         const double *t2, int64_t p, int64_t h, double *l1, double *l2,
-                         nlb_stream_t stream);
+int nlb_pppp_ladders_f64(const nlb_pppp_plan *plan, const double *t1, const double *t2, int64_t p, int64_t h,
+                         double *l1, double *l2, nlb_stream_t stream);
 
 /* Jacobi steps with mixing for T1 and T2 (coupled_cluster.py:410-414,
  * 538-545, 614-620); e1/e2 (optional) receive new - old. */
@@ -358,15 +391,20 @@ int nlb_jacobi_f64(const double *t1, const double *H1, const double *t2, const d
                    int64_t p, int64_t h, double mixing, double *t1_out, double *t2_out, double *e1,
                    double *e2, nlb_stream_t stream);
 
+/* Doubles of the `work` buffer of nlb_dense_energy_f64 and nlb_vec_diis_f64
+ * (per-block partial sums, added in a fixed order). */
+#define NLB_DENSE_WORK_DOUBLES 57344
+
 /* ccsd_energy (coupled_cluster.py:265-286) into *out (device); v_pphh may be
- * NULL when it is zero. */
+ * NULL when it is zero.  work holds NLB_DENSE_WORK_DOUBLES doubles. */
 int nlb_dense_energy_f64(const double *f_ph, const double *t1, const double *v_pphh,
-                         const double *t2, int64_t p, int64_t h, double *out, nlb_stream_t stream);
+                         const double *t2, int64_t p, int64_t h, double *out, double *work,
+                         nlb_stream_t stream);
 
 /* Pulsed DIIS on concatenated amplitude vectors (soa/coupled_cluster.py:
  * 533-561): Gram of m error vectors err[m][n], FP64 bordered solve, and
  * out = sum_s c_s hist[s] (out untouched when the solve fails).  work holds
- * 512 doubles. */
+ * NLB_DENSE_WORK_DOUBLES doubles. */
 int nlb_vec_diis_f64(const double *err, const double *hist, int64_t n, int32_t m, double *work,
                      double *out, nlb_stream_t stream);
 

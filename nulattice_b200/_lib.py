@@ -87,6 +87,21 @@ class ContractDesc(ctypes.Structure):
                                            "sa_k", "sb_k", "sa_b", "sb_b", "sc_b")]
 
 
+class PpphPlan(ctypes.Structure):
+    _fields_ = [("nnz", c_int64), ("idx", c_void_p), ("val", c_void_p),
+                ("perm_adk", c_void_p), ("perm_ak", c_void_p), ("perm_cdk", c_void_p)] + \
+               [(n, c_int64) for n in ("n_a", "n_ad", "n_adk", "n_ak", "n_cdk")] + \
+               [(n, c_void_p) for n in ("seg_a", "seg_ad", "seg_adk", "seg_ak", "seg_cdk")]
+
+
+class PpppPlan(ctypes.Structure):
+    _fields_ = [("nnz", c_int64), ("idx", c_void_p), ("val", c_void_p), ("perm_ab", c_void_p),
+                ("n_ab", c_int64), ("seg_ab", c_void_p)]
+
+
+NLB_DENSE_WORK_DOUBLES = 57344
+
+
 class PwProblem(ctypes.Structure):
     _fields_ = [("L", c_int32), ("n_blocks", c_int32), ("n_pmom", c_int32), ("n_hmom", c_int32),
                 ("n_t2", c_int64), ("n_m", c_int64), ("n_w", c_int64), ("n_rows", c_int64),
@@ -150,12 +165,13 @@ def lib():
     L.nlb_contract_gemm_f64.argtypes = [ctypes.POINTER(ContractDesc), c_void_p, c_void_p, c_void_p, c_double,
                                         c_double, c_void_p, c_int64, c_void_p]
     L.nlb_antisym_acc_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int64, c_int32, c_double, c_void_p]
-    L.nlb_ppph_intermediates_f64.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_int64,
+    L.nlb_ppph_intermediates_f64.argtypes = [ctypes.POINTER(PpphPlan), c_void_p, c_void_p, c_int64, c_int64,
                                              c_void_p, c_void_p]
-    L.nlb_pppp_ladders_f64.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_int64,
+    L.nlb_pppp_ladders_f64.argtypes = [ctypes.POINTER(PpppPlan), c_void_p, c_void_p, c_int64, c_int64,
                                        c_void_p, c_void_p, c_void_p]
     L.nlb_jacobi_f64.argtypes = [c_void_p] * 8 + [c_int64, c_int64, c_double] + [c_void_p] * 5
-    L.nlb_dense_energy_f64.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]
+    L.nlb_dense_energy_f64.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p,
+                                       c_void_p, c_void_p]
     L.nlb_lambda_acc_len.argtypes = [ctypes.POINTER(StructProblem)]
     L.nlb_lambda_acc_len.restype = c_int64
     L.nlb_lambda_gb_len.argtypes = [ctypes.POINTER(StructProblem)]

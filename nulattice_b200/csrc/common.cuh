@@ -40,8 +40,26 @@ __device__ double block_sum(double v) {
 //   xc[n_xc]    Xh2[H_g[k'], H_g[i']] per label (k' major)
 //   dpc[p]      dXp2 in label order
 //   dhc[h]      diag Xh2 in label order
+//   red[kRedLen] per-block partial sums of the reductions of a step (below)
+//
+// Reductions are deterministic: a kernel that reduces over the grid writes
+// one partial per block into its own slot range of `red`, and the kernel that
+// consumes the total (k_finish, k_l_finish, the DIIS Gram reduction) adds the
+// partials in slot order.  No floating-point atomics, so a solve repeats bit
+// for bit and its stopping step does not depend on block scheduling.
+constexpr int kRedSlots = 2048;            // most blocks of a reducing launch
+constexpr int kRedKinds = 4;               // partial arrays of kRedSlots each
+constexpr int kGramSlots = 512;            // most blocks of the DIIS Gram launch
+constexpr int kGramPairs = 55;             // pairs (s <= t) of at most 10 vectors
+constexpr int64_t kRedLen = (int64_t)kRedKinds * kRedSlots + (int64_t)kGramSlots * kGramPairs;
+// slot ranges of `red`: the forward step uses E, DT1, DT2; the Lambda step
+// uses NRM1 (|lam1|^2), DT1, DT2 and NRM2 (|Lam|^2)
+enum { kRedE = 0, kRedNrm1 = 0, kRedDt1 = 1, kRedDt2 = 2, kRedNrm2 = 3 };
+
 struct PrepView {
-    double *Q, *Xh2, *Xh1, *dXp2, *dXp1, *t1c, *xc, *dpc, *dhc;
+    double *Q, *Xh2, *Xh1, *dXp2, *dXp1, *t1c, *xc, *dpc, *dhc, *red;
+    __host__ __device__ double* slots(int kind) const { return red + (int64_t)kind * kRedSlots; }
+    __host__ __device__ double* gram_slots() const { return red + (int64_t)kRedKinds * kRedSlots; }
 };
 
 __host__ __device__ inline PrepView prep_view(double* base, const nlb_struct_problem& P) {
@@ -56,7 +74,18 @@ __host__ __device__ inline PrepView prep_view(double* base, const nlb_struct_pro
     v.xc = v.t1c + P.n_t1c;
     v.dpc = v.xc + P.n_xc;
     v.dhc = v.dpc + P.p;
+    v.red = v.dhc + P.h;
     return v;
+}
+
+// Sum of the first n partials at `part` in a fixed order: lane-strided
+// sums, then a fixed butterfly.  Every lane of the (full) warp must call it
+// with the same n; all lanes return the same value.
+__device__ __forceinline__ double warp_sum_slots(const double* part, int n) {
+    double s = 0.0;
+    for (int b = (int)(threadIdx.x & 31); b < n; b += 32) s += part[b];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
 }
 
 __device__ __forceinline__ int find_label(const int32_t* base, int G, int64_t u) {

@@ -39,6 +39,10 @@ int dcheck(const char* where) {
 }
 
 constexpr int TM = 64, TN = 64, TK = 16;
+// most blocks of a reducing launch (partials in the caller's work buffer,
+// NLB_DENSE_WORK_DOUBLES = 512 + kDenseSlots * 55)
+constexpr int kDenseSlots = 1024;
+static_assert(512 + kDenseSlots * 55 <= NLB_DENSE_WORK_DOUBLES, "work buffer");
 
 __device__ __forceinline__ int64_t decode(int64_t lin, const int64_t* ext, const int64_t* str, int nd) {
     int64_t off = 0;
@@ -184,44 +188,110 @@ __global__ void k_antisym_diag(double* H, int64_t p, int64_t h) {
 }
 
 // The seven v_ppph intermediates of CCM/ccDgrams.py:13-45 from the row list
-// (c, d, a, k, v): one thread per (entry, hole pair).  Outputs are zeroed by
-// the caller; repeated keys add up through the atomics.
-__global__ void k_ppph(const int64_t* __restrict__ idx, const double* __restrict__ val, int64_t nnz,
-                       const double* __restrict__ t1, const double* __restrict__ t2, int64_t p, int64_t h,
-                       double* r0, double* r1, double* r2, double* r3, double* r4, double* r5, double* r6) {
-    const int64_t hh = h * h;
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nnz * hh;
-         u += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t q = u / hh, ij = u % hh, i = ij / h, j = ij % h;
-        const int64_t c = idx[4 * q], dd = idx[4 * q + 1], a = idx[4 * q + 2], k = idx[4 * q + 3];
-        const double v = val[q];
-        if (ij == 0) {
-            atomicAdd(&r1[a * p + dd], -v * t1[c * h + k]);
-            atomicAdd(&r3[dd * p + a], v * t1[c * h + k]);
+// (c, d, a, k, v).  Deterministic gathers: the plan holds the list sorted by
+// each output's key (stable, so repeated keys keep their list order), and one
+// thread per (key segment, free hole indices) adds the segment's terms in that
+// order into the output it alone owns.  Outputs are zeroed by the caller.
+struct PpphEntry {
+    int64_t c, d, a, k;
+    double v;
+};
+
+__device__ __forceinline__ PpphEntry ppph_entry(const nlb_ppph_plan& P, const int32_t* perm, int64_t q) {
+    const int64_t e = perm[q];
+    return PpphEntry{P.idx[4 * e], P.idx[4 * e + 1], P.idx[4 * e + 2], P.idx[4 * e + 3], P.val[e]};
+}
+
+// r1[a,d] -= v t1[c,k] and r3[d,a] += v t1[c,k]: one thread per (a, d) segment
+__global__ void k_ppph_ad(nlb_ppph_plan P, const double* __restrict__ t1, int64_t p, int64_t h, double* r1,
+                          double* r3) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < P.n_ad; s += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        PpphEntry e{};
+        for (int64_t q = P.seg_ad[s]; q < P.seg_ad[s + 1]; ++q) {
+            e = ppph_entry(P, P.perm_adk, q);
+            acc += e.v * t1[e.c * h + e.k];
         }
-        if (i == 0) {
-            // j plays the free hole index here
-            atomicAdd(&r0[a * h + j], -0.5 * v * t2[((c * p + dd) * h + k) * h + j]);
-            atomicAdd(&r2[((c * p + dd) * h + j) * h + k], v * t1[a * h + j]);
-            atomicAdd(&r4[((a * p + dd) * h + j) * h + k], v * t1[c * h + j]);
-        }
-        atomicAdd(&r5[((a * h + i) * h + j) * h + k], v * t2[((c * p + dd) * h + i) * h + j]);
-        atomicAdd(&r6[((a * h + i) * h + j) * h + k], v * t1[c * h + i] * t1[dd * h + j]);
+        r1[e.a * p + e.d] -= acc;
+        r3[e.d * p + e.a] += acc;
     }
 }
 
-// The two v_pppp ladders of CCM/ccDgrams.py:215-237 (without the 1/2).
-__global__ void k_pppp(const int64_t* __restrict__ idx, const double* __restrict__ val, int64_t nnz,
-                       const double* __restrict__ t1, const double* __restrict__ t2, int64_t p, int64_t h,
-                       double* l1, double* l2) {
+// r0[a,j] -= 1/2 v t2[c,d,k,j]: one thread per (a segment, j)
+__global__ void k_ppph_a(nlb_ppph_plan P, const double* __restrict__ t2, int64_t p, int64_t h, double* r0) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_a * h; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = u / h, j = u - s * h;
+        double acc = 0.0;
+        PpphEntry e{};
+        for (int64_t q = P.seg_a[s]; q < P.seg_a[s + 1]; ++q) {
+            e = ppph_entry(P, P.perm_adk, q);
+            acc += e.v * t2[((e.c * p + e.d) * h + e.k) * h + j];
+        }
+        r0[e.a * h + j] -= 0.5 * acc;
+    }
+}
+
+// r4[a,d,j,k] += v t1[c,j]: per (a, d, k) segment and j (list order A);
+// r2[c,d,j,k] += v t1[a,j]: per (c, d, k) segment and j (list order C)
+__global__ void k_ppph_r24(nlb_ppph_plan P, const double* __restrict__ t1, int64_t p, int64_t h, double* r2,
+                           double* r4) {
+    const int64_t n4 = P.n_adk * h, n2 = P.n_cdk * h;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n4 + n2; u += (int64_t)gridDim.x * blockDim.x) {
+        const bool four = u < n4;
+        const int64_t v = four ? u : u - n4;
+        const int64_t s = v / h, j = v - s * h;
+        const int64_t* seg = four ? P.seg_adk : P.seg_cdk;
+        const int32_t* perm = four ? P.perm_adk : P.perm_cdk;
+        double acc = 0.0;
+        PpphEntry e{};
+        for (int64_t q = seg[s]; q < seg[s + 1]; ++q) {
+            e = ppph_entry(P, perm, q);
+            acc += e.v * t1[(four ? e.c : e.a) * h + j];
+        }
+        if (four) r4[((e.a * p + e.d) * h + j) * h + e.k] += acc;
+        else r2[((e.c * p + e.d) * h + j) * h + e.k] += acc;
+    }
+}
+
+// r5[a,i,j,k] += v t2[c,d,i,j] and r6[a,i,j,k] += v t1[c,i] t1[d,j]: one
+// thread per (a, k) segment and hole pair (i, j)
+__global__ void k_ppph_ak(nlb_ppph_plan P, const double* __restrict__ t1, const double* __restrict__ t2, int64_t p,
+                          int64_t h, double* r5, double* r6) {
     const int64_t hh = h * h;
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nnz * hh;
-         u += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t q = u / hh, ij = u % hh, i = ij / h, j = ij % h;
-        const int64_t a = idx[4 * q], b = idx[4 * q + 1], c = idx[4 * q + 2], dd = idx[4 * q + 3];
-        const double v = val[q];
-        atomicAdd(&l1[(a * p + b) * hh + ij], v * t2[(c * p + dd) * hh + ij]);
-        atomicAdd(&l2[(a * p + b) * hh + ij], v * t1[c * h + i] * t1[dd * h + j]);
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_ak * hh; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = u / hh, ij = u - s * hh, i = ij / h, j = ij - i * h;
+        double a5 = 0.0, a6 = 0.0;
+        PpphEntry e{};
+        for (int64_t q = P.seg_ak[s]; q < P.seg_ak[s + 1]; ++q) {
+            e = ppph_entry(P, P.perm_ak, q);
+            a5 += e.v * t2[(e.c * p + e.d) * hh + ij];
+            a6 += e.v * t1[e.c * h + i] * t1[e.d * h + j];
+        }
+        r5[((e.a * h + i) * h + j) * h + e.k] += a5;
+        r6[((e.a * h + i) * h + j) * h + e.k] += a6;
+    }
+}
+
+// The two v_pppp ladders of CCM/ccDgrams.py:215-237 (without the 1/2): one
+// thread per ((a, b) segment, hole pair), terms in list order.
+__global__ void k_pppp(nlb_pppp_plan P, const double* __restrict__ t1, const double* __restrict__ t2, int64_t p,
+                       int64_t h, double* l1, double* l2) {
+    const int64_t hh = h * h;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_ab * hh; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = u / hh, ij = u - s * hh, i = ij / h, j = ij - i * h;
+        double a1 = 0.0, a2 = 0.0;
+        int64_t a = 0, b = 0;
+        for (int64_t q = P.seg_ab[s]; q < P.seg_ab[s + 1]; ++q) {
+            const int64_t e = P.perm_ab[q];
+            a = P.idx[4 * e];
+            b = P.idx[4 * e + 1];
+            const int64_t c = P.idx[4 * e + 2], dd = P.idx[4 * e + 3];
+            const double v = P.val[e];
+            a1 += v * t2[(c * p + dd) * hh + ij];
+            a2 += v * t1[c * h + i] * t1[dd * h + j];
+        }
+        l1[(a * p + b) * hh + ij] += a1;
+        l2[(a * p + b) * hh + ij] += a2;
     }
 }
 
@@ -266,9 +336,9 @@ __device__ double dblock_sum(double v) {
 }
 
 // E = sum f_ai t1_ai + 1/4 sum v_abij t2_abij + 1/2 sum v_abij t1_ai t1_bj
-// (coupled_cluster.py:265-286), accumulated into *out.
+// (coupled_cluster.py:265-286): one partial per block into part[blockIdx.x].
 __global__ void k_energy_dense(const double* f_ph, const double* t1, const double* v, const double* t2, int64_t p,
-                               int64_t h, double* out) {
+                               int64_t h, double* part) {
     double acc = 0.0;
     const int64_t n1 = p * h, n2 = p * p * h * h;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n1 + n2;
@@ -282,12 +352,21 @@ __global__ void k_energy_dense(const double* f_ph, const double* t1, const doubl
         }
     }
     const double s = dblock_sum(acc);
-    if (threadIdx.x == 0) atomicAdd(out, s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
-// Gram matrix <e_s, e_t> of m stored error vectors, accumulated into gram
-// (row stride 16).
-__global__ void k_vec_gram(const double* E, int64_t n, int m, double* gram) {
+// *out = the n partials at `part` added in slot order (one warp, fixed tree).
+__global__ void k_sum_part(const double* part, int n, double* out) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < n; b += 32) s += part[b];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// Gram matrix <e_s, e_t> of m stored error vectors: per-block partials of
+// the pairs s <= t into part[blockIdx.x * 55 + k]; k_vec_gram_reduce adds them
+// in block order into gram (row stride 16).
+__global__ void k_vec_gram(const double* E, int64_t n, int m, double* part) {
     double acc[55];
     for (int k = 0; k < 55; ++k) acc[k] = 0.0;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -297,12 +376,24 @@ __global__ void k_vec_gram(const double* E, int64_t n, int m, double* gram) {
         for (int s = 0; s < m; ++s)
             for (int t = s; t < m; ++t) acc[k++] += v[s] * v[t];
     }
-    int k = 0;
-    for (int s = 0; s < m; ++s)
-        for (int t = s; t < m; ++t) {
-            const double tot = dblock_sum(acc[k++]);
-            if (threadIdx.x == 0) atomicAdd(&gram[s * 16 + t], tot);
-        }
+    const int np = m * (m + 1) / 2;
+    for (int k = 0; k < np; ++k) {
+        const double tot = dblock_sum(acc[k]);
+        if (threadIdx.x == 0) part[(int64_t)blockIdx.x * 55 + k] = tot;
+    }
+}
+
+// One block per pair k of the upper triangle: its nb partials in block order.
+__global__ void k_vec_gram_reduce(const double* part, int nb, int m, double* gram) {
+    const int k = blockIdx.x;
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += part[(int64_t)b * 55 + k];
+    acc = dblock_sum(acc);
+    if (threadIdx.x == 0) {
+        int s = 0, rem = k;
+        while (rem >= m - s) { rem -= m - s; ++s; }
+        gram[s * 16 + s + rem] = acc;
+    }
 }
 
 // Pulsed DIIS extrapolation (soa/coupled_cluster.py:533-561): bordered system
@@ -481,20 +572,32 @@ int nlb_antisym_project_f64(double* H, int64_t p, int64_t h, nlb_stream_t stream
     return dcheck("nlb_antisym_project_f64");
 }
 
-int nlb_ppph_intermediates_f64(const int64_t* idx, const double* val, int64_t nnz, const double* t1,
-                               const double* t2, int64_t p, int64_t h, double* const* r, nlb_stream_t stream) {
-    if (nnz == 0) return NLB_OK;
-    if (!idx || !val || !t1 || !t2 || !r) return dfail(NLB_ERR_ARG, "nlb_ppph_intermediates_f64: null argument");
-    k_ppph<<<grid1(nnz * h * h), 256, 0, (cudaStream_t)stream>>>(idx, val, nnz, t1, t2, p, h, r[0], r[1], r[2], r[3],
-                                                                  r[4], r[5], r[6]);
+int nlb_ppph_intermediates_f64(const nlb_ppph_plan* plan, const double* t1, const double* t2, int64_t p,
+                               int64_t h, double* const* r, nlb_stream_t stream) {
+    if (!plan) return dfail(NLB_ERR_ARG, "nlb_ppph_intermediates_f64: null plan");
+    if (plan->nnz == 0) return NLB_OK;
+    const nlb_ppph_plan& P = *plan;
+    if (!P.idx || !P.val || !P.perm_adk || !P.perm_ak || !P.perm_cdk || !P.seg_a || !P.seg_ad || !P.seg_adk ||
+        !P.seg_ak || !P.seg_cdk || !t1 || !t2 || !r)
+        return dfail(NLB_ERR_ARG, "nlb_ppph_intermediates_f64: null argument");
+    if (P.n_a < 0 || P.n_ad < 0 || P.n_adk < 0 || P.n_ak < 0 || P.n_cdk < 0 || p <= 0 || h <= 0)
+        return dfail(NLB_ERR_SIZE, "nlb_ppph_intermediates_f64: bad sizes");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (P.n_ad) k_ppph_ad<<<grid1(P.n_ad), 256, 0, s>>>(P, t1, p, h, r[1], r[3]);
+    if (P.n_a) k_ppph_a<<<grid1(P.n_a * h), 256, 0, s>>>(P, t2, p, h, r[0]);
+    if (P.n_adk + P.n_cdk) k_ppph_r24<<<grid1((P.n_adk + P.n_cdk) * h), 256, 0, s>>>(P, t1, p, h, r[2], r[4]);
+    if (P.n_ak) k_ppph_ak<<<grid1(P.n_ak * h * h), 256, 0, s>>>(P, t1, t2, p, h, r[5], r[6]);
     return dcheck("nlb_ppph_intermediates_f64");
 }
 
-int nlb_pppp_ladders_f64(const int64_t* idx, const double* val, int64_t nnz, const double* t1, const double* t2,
-                         int64_t p, int64_t h, double* l1, double* l2, nlb_stream_t stream) {
-    if (nnz == 0) return NLB_OK;
-    if (!idx || !val || !t1 || !t2 || !l1 || !l2) return dfail(NLB_ERR_ARG, "nlb_pppp_ladders_f64: null argument");
-    k_pppp<<<grid1(nnz * h * h), 256, 0, (cudaStream_t)stream>>>(idx, val, nnz, t1, t2, p, h, l1, l2);
+int nlb_pppp_ladders_f64(const nlb_pppp_plan* plan, const double* t1, const double* t2, int64_t p, int64_t h,
+                         double* l1, double* l2, nlb_stream_t stream) {
+    if (!plan) return dfail(NLB_ERR_ARG, "nlb_pppp_ladders_f64: null plan");
+    if (plan->nnz == 0 || plan->n_ab == 0) return NLB_OK;
+    if (!plan->idx || !plan->val || !plan->perm_ab || !plan->seg_ab || !t1 || !t2 || !l1 || !l2)
+        return dfail(NLB_ERR_ARG, "nlb_pppp_ladders_f64: null argument");
+    if (plan->n_ab < 0 || p <= 0 || h <= 0) return dfail(NLB_ERR_SIZE, "nlb_pppp_ladders_f64: bad sizes");
+    k_pppp<<<grid1(plan->n_ab * h * h), 256, 0, (cudaStream_t)stream>>>(*plan, t1, t2, p, h, l1, l2);
     return dcheck("nlb_pppp_ladders_f64");
 }
 
@@ -509,11 +612,14 @@ int nlb_jacobi_f64(const double* t1, const double* H1, const double* t2, const d
 }
 
 int nlb_dense_energy_f64(const double* f_ph, const double* t1, const double* v_pphh, const double* t2, int64_t p,
-                         int64_t h, double* out, nlb_stream_t stream) {
-    if (!f_ph || !t1 || !out) return dfail(NLB_ERR_ARG, "nlb_dense_energy_f64: null argument");
+                         int64_t h, double* out, double* work, nlb_stream_t stream) {
+    if (!f_ph || !t1 || !out || !work) return dfail(NLB_ERR_ARG, "nlb_dense_energy_f64: null argument");
+    if (v_pphh && !t2) return dfail(NLB_ERR_ARG, "nlb_dense_energy_f64: v_pphh without t2");
     cudaStream_t s = (cudaStream_t)stream;
-    cudaMemsetAsync(out, 0, sizeof(double), s);
-    k_energy_dense<<<grid1(p * h + (v_pphh ? p * p * h * h : 0)), 256, 0, s>>>(f_ph, t1, v_pphh, t2, p, h, out);
+    int nb = grid1(p * h + (v_pphh ? p * p * h * h : 0));
+    if (nb > kDenseSlots) nb = kDenseSlots;
+    k_energy_dense<<<nb, 256, 0, s>>>(f_ph, t1, v_pphh, t2, p, h, work);
+    k_sum_part<<<1, 32, 0, s>>>(work, nb, out);
     return dcheck("nlb_dense_energy_f64");
 }
 
@@ -521,8 +627,12 @@ int nlb_vec_diis_f64(const double* err, const double* hist, int64_t n, int32_t m
                      nlb_stream_t stream) {
     if (!err || !hist || !work || !out || m < 1 || m > 10) return dfail(NLB_ERR_ARG, "nlb_vec_diis_f64: bad argument");
     cudaStream_t s = (cudaStream_t)stream;
-    cudaMemsetAsync(work, 0, 16 * 16 * sizeof(double), s);
-    k_vec_gram<<<grid1(n), 256, 0, s>>>(err, n, m, work);
+    // work: gram [0, 256), coefficients [256, 512), Gram partials after that
+    int nb = grid1(n);
+    if (nb > kDenseSlots) nb = kDenseSlots;
+    double* part = work + 512;
+    k_vec_gram<<<nb, 256, 0, s>>>(err, n, m, part);
+    k_vec_gram_reduce<<<m * (m + 1) / 2, 256, 0, s>>>(part, nb, m, work);
     k_vec_diis_solve<<<1, 32, 0, s>>>(work, m, work + 256);
     k_vec_combine<<<grid1(n), 256, 0, s>>>(work + 256, hist, n, m, out);
     return dcheck("nlb_vec_diis_f64");

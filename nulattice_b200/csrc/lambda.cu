@@ -269,8 +269,8 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
     const double s1 = block_sum(dnrm);
     const double s2 = block_sum(lnrm);
     if (tid == 0) {
-        atomicAdd(&S.ctrl->dt2_sq, 4.0 * s1);
-        atomicAdd(&S.ctrl->e_acc, 4.0 * s2);
+        PV.slots(kRedDt2)[blockIdx.x] = 4.0 * s1;
+        PV.slots(kRedNrm2)[blockIdx.x] = 4.0 * s2;
     }
 }
 
@@ -353,15 +353,25 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
     const double s1 = block_sum(dn);
     const double s2 = block_sum(ln);
     if (threadIdx.x == 0) {
-        atomicAdd(&c->dt1_sq, s1);
-        atomicAdd(&c->e_acc, s2);
+        PV.slots(kRedDt1)[blockIdx.x] = s1;
+        PV.slots(kRedNrm1)[blockIdx.x] = s2;
     }
 }
 
 // Convergence on the relative step of the multipliers; DIIS bookkeeping as
 // in the forward k_finish (a pulse when max_diis error vectors are stored).
-__global__ void k_l_finish(nlb_ctrl* c) {
-    if (threadIdx.x != 0 || blockIdx.x != 0 || c->status != NLB_RUNNING) return;
+// One warp: the norms from the per-block partials of the T1 (n1 blocks) and
+// row (n2 blocks) launches, added in slot order.
+__global__ void k_l_finish(nlb_ctrl* c, const double* red, int n1, int n2) {
+    if (blockIdx.x != 0 || c->status != NLB_RUNNING) return;
+    const double d1 = warp_sum_slots(red + (int64_t)kRedDt1 * kRedSlots, n1);
+    const double l1 = warp_sum_slots(red + (int64_t)kRedNrm1 * kRedSlots, n1);
+    const double d2 = warp_sum_slots(red + (int64_t)kRedDt2 * kRedSlots, n2);
+    const double l2 = warp_sum_slots(red + (int64_t)kRedNrm2 * kRedSlots, n2);
+    if (threadIdx.x != 0) return;
+    c->dt1_sq = d1;
+    c->dt2_sq = d2;
+    c->e_acc = l1 + l2;
     c->iter += 1;
     c->parity ^= 1;
     c->diis_pulse = 0;
@@ -381,9 +391,6 @@ __global__ void k_l_finish(nlb_ctrl* c) {
         }
         if (c->iter >= c->max_steps) c->status = NLB_MAX_ITER;
     }
-    c->dt1_sq = 0.0;
-    c->dt2_sq = 0.0;
-    c->e_acc = 0.0;
 }
 
 __global__ void k_l_init(nlb_ctrl* c, double tol, double mixing, int max_steps, int max_diis) {
@@ -418,7 +425,13 @@ __global__ void k_l_coupling(nlb_struct_problem P, nlb_lambda_state S, const dou
         acc += Lm[u] * (dw[ch.hh_ptr_off + hp] + dv[ch.pp_ptr_off + ab]) * tau;
     }
     const double s = block_sum(acc);
-    if (threadIdx.x == 0) atomicAdd(out, s);
+    if (threadIdx.x == 0) PV.slots(0)[blockIdx.x] = s;
+}
+
+// *out = the n per-block partials at `part`, added in slot order (one warp).
+__global__ void k_l_sum_slots(const double* part, int n, double* out) {
+    const double s = warp_sum_slots(part, n);
+    if (threadIdx.x == 0) *out = s;
 }
 
 // ======================================================== lattice path ==
@@ -894,8 +907,8 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
     const double s1 = block_sum(dnrm);
     const double s2 = block_sum(lnrm);
     if (tid == 0) {
-        atomicAdd(&S.ctrl->dt2_sq, 4.0 * s1);
-        atomicAdd(&S.ctrl->e_acc, 4.0 * s2);
+        PV.slots(kRedDt2)[blockIdx.x] = 4.0 * s1;
+        PV.slots(kRedNrm2)[blockIdx.x] = 4.0 * s2;
     }
 }
 
@@ -981,13 +994,16 @@ int col_chunks(const nlb_struct_problem* P) {
 }
 
 template <typename T, int NT, int MINB>
-void launch_llat(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_t s) {
+int launch_llat(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_t s) {
     const int64_t sm = llat_smem(P->max_row, NT / kLHP, sizeof(T)).total;
     auto kern = k_l_lat<T, NT, MINB>;
     const int bps = lat_bps(reinterpret_cast<const void*>(kern), sm, NT);
     int64_t grid = (int64_t)num_sms_l() * bps;
     if (grid > P->n_rows) grid = P->n_rows;
+    if (grid > kRedSlots) grid = kRedSlots;
+    if (grid < 1) grid = 1;
     kern<<<(unsigned)grid, NT, (size_t)sm, s>>>(*P, *S);
+    return (int)grid;
 }
 
 template <typename T>
@@ -1010,15 +1026,17 @@ int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_
         k_l_cols<T, kColThreads><<<(unsigned)items, kColThreads, 0, s>>>(*P, *S, nchunk);
     }
     // row-pass launch shape from the tuning word (bits 4-7)
+    int n2 = 0;
     if constexpr (sizeof(T) == 4) {
-        if (((P->tune >> 4) & 15) == 1) launch_llat<T, 512, 1>(P, S, s);
-        else launch_llat<T, kLatThreads, MINB>(P, S, s);
+        if (((P->tune >> 4) & 15) == 1) n2 = launch_llat<T, 512, 1>(P, S, s);
+        else n2 = launch_llat<T, kLatThreads, MINB>(P, S, s);
     } else {
-        launch_llat<T, kLatThreads, MINB>(P, S, s);
+        n2 = launch_llat<T, kLatThreads, MINB>(P, S, s);
     }
     if (cudaPeekAtLastError() != cudaSuccess) return lcheck("nlb_lambda_step");
-    k_l_t1<<<grid_l((int64_t)P->p * P->h), kThreads, 0, s>>>(*P, *S);
-    k_l_finish<<<1, 32, 0, s>>>(S->ctrl);
+    const int n1 = grid_l((int64_t)P->p * P->h);
+    k_l_t1<<<n1, kThreads, 0, s>>>(*P, *S);
+    k_l_finish<<<1, 32, 0, s>>>(S->ctrl, prep_view(S->prep, *P).red, n1, n2);
     return lcheck("nlb_lambda_step");
 }
 
@@ -1090,10 +1108,12 @@ int nlb_lambda_step(const nlb_struct_problem* prob, const nlb_lambda_state* st, 
     const int bps = lat_bps(reinterpret_cast<const void*>(k_l_rows), sm, kThreads);
     int64_t grid = (int64_t)num_sms_l() * bps;
     if (grid > prob->n_rows) grid = prob->n_rows;
+    if (grid > kRedSlots) grid = kRedSlots;
     if (grid < 1) grid = 1;
     k_l_rows<<<(unsigned)grid, kThreads, (size_t)sm, s>>>(*prob, *st);
-    k_l_t1<<<grid_l((int64_t)prob->p * prob->h), kThreads, 0, s>>>(*prob, *st);
-    k_l_finish<<<1, 32, 0, s>>>(st->ctrl);
+    const int n1 = grid_l((int64_t)prob->p * prob->h);
+    k_l_t1<<<n1, kThreads, 0, s>>>(*prob, *st);
+    k_l_finish<<<1, 32, 0, s>>>(st->ctrl, prep_view(st->prep, *prob).red, n1, (int)grid);
     return lcheck("nlb_lambda_step");
 }
 
@@ -1120,9 +1140,11 @@ int nlb_lambda_coupling(const nlb_struct_problem* prob, const nlb_lambda_state* 
                         const double* dv, double* out, nlb_stream_t stream) {
     if (!prob || !st || !dw || !dv || !out) return lfail(NLB_ERR_ARG, "nlb_lambda_coupling: null argument");
     if (st->dtype != NLB_F64) return lfail(NLB_ERR_ARG, "nlb_lambda_coupling: needs the FP64 state");
+    if (!st->prep) return lfail(NLB_ERR_ARG, "nlb_lambda_coupling: null prep");
     cudaStream_t s = (cudaStream_t)stream;
-    cudaMemsetAsync(out, 0, sizeof(double), s);
-    k_l_coupling<<<grid_l(prob->n_t2), kThreads, 0, s>>>(*prob, *st, dw, dv, out);
+    const int nb = grid_l(prob->n_t2);
+    k_l_coupling<<<nb, kThreads, 0, s>>>(*prob, *st, dw, dv, out);
+    k_l_sum_slots<<<1, 32, 0, s>>>(prep_view(st->prep, *prob).slots(0), nb, out);
     return lcheck("nlb_lambda_coupling");
 }
 

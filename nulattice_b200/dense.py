@@ -223,6 +223,67 @@ def _rows_dev(x, dev):
             torch.as_tensor(np.ascontiguousarray(val, dtype=np.float64), device=dev), len(val))
 
 
+def _key_order(*cols):
+    """Stable order of the rows by the key columns (first column primary) and
+    the starts of the runs of equal keys (with the end appended)."""
+    n = len(cols[0])
+    order = np.lexsort((np.arange(n),) + tuple(reversed(cols)))
+    if n == 0:
+        return order.astype(np.int32), np.zeros(1, np.int64)
+    srt = np.stack([c[order] for c in cols], axis=1)
+    change = np.concatenate([[True], np.any(srt[1:] != srt[:-1], axis=1)])
+    starts = np.flatnonzero(change)
+    return order.astype(np.int32), np.concatenate([starts, [n]]).astype(np.int64)
+
+
+def _runs(order, cols):
+    """Starts (with the end) of the runs of equal keys of `cols` in `order`."""
+    n = len(order)
+    if n == 0:
+        return np.zeros(1, np.int64)
+    srt = np.stack([c[order] for c in cols], axis=1)
+    change = np.concatenate([[True], np.any(srt[1:] != srt[:-1], axis=1)])
+    return np.concatenate([np.flatnonzero(change), [n]]).astype(np.int64)
+
+
+class _SparsePlan:
+    """A v_ppph / v_pppp row list on the device with the orders its
+    contractions gather in (``nlb_ppph_plan`` / ``nlb_pppp_plan``): every
+    output entry sums its rows in one fixed order, so results repeat bit for
+    bit."""
+
+    def __init__(self, rows, kind, dev):
+        idx_d, val_d, nnz = rows
+        self.nnz = nnz
+        self.keep = [idx_d, val_d]
+        idx = idx_d.cpu().numpy().reshape(-1, 4) if nnz else np.zeros((0, 4), np.int64)
+        dv = lambda a: self._dev(a, dev)  # noqa: E731
+        if kind == "ppph":
+            c, d, a, k = idx.T
+            perm_adk, seg_adk = _key_order(a, d, k)
+            seg_a, seg_ad = _runs(perm_adk, (a,)), _runs(perm_adk, (a, d))
+            perm_ak, seg_ak = _key_order(a, k)
+            perm_cdk, seg_cdk = _key_order(c, d, k)
+            self.c = _lib.PpphPlan(nnz=nnz, idx=idx_d.data_ptr() if nnz else None,
+                                   val=val_d.data_ptr() if nnz else None,
+                                   perm_adk=dv(perm_adk), perm_ak=dv(perm_ak), perm_cdk=dv(perm_cdk),
+                                   n_a=len(seg_a) - 1, n_ad=len(seg_ad) - 1, n_adk=len(seg_adk) - 1,
+                                   n_ak=len(seg_ak) - 1, n_cdk=len(seg_cdk) - 1,
+                                   seg_a=dv(seg_a), seg_ad=dv(seg_ad), seg_adk=dv(seg_adk), seg_ak=dv(seg_ak),
+                                   seg_cdk=dv(seg_cdk))
+        else:
+            a, b = idx[:, 0], idx[:, 1]
+            perm_ab, seg_ab = _key_order(a, b)
+            self.c = _lib.PpppPlan(nnz=nnz, idx=idx_d.data_ptr() if nnz else None,
+                                   val=val_d.data_ptr() if nnz else None, perm_ab=dv(perm_ab),
+                                   n_ab=len(seg_ab) - 1, seg_ab=dv(seg_ab))
+
+    def _dev(self, a, dev):
+        t = torch.as_tensor(np.ascontiguousarray(a if len(a) else np.zeros(1, a.dtype)), device=dev)
+        self.keep.append(t)
+        return t.data_ptr()
+
+
 class DenseEngine:
     def __init__(self, fock_mats, two_body_int, dev):
         self.dev = dev
@@ -255,8 +316,10 @@ class DenseEngine:
             vd = _dense_block(v_pppp, (p, p, p, p), dev)
             if int(torch.count_nonzero(vd).item()) * DENSE_PPPP_FRACTION >= vd.numel():
                 self.pppp_dense = vd
-        self.pppp = self._sparse(v_pppp, (p, p, p, p)) if self.pppp_dense is None else (None, None, 0)
-        self.ppph = self._sparse(v_ppph, (p, p, p, h))
+        self.pppp = _SparsePlan(self._sparse(v_pppp, (p, p, p, p)) if self.pppp_dense is None else (None, None, 0),
+                                "pppp", dev)
+        self.ppph = _SparsePlan(self._sparse(v_ppph, (p, p, p, h)), "ppph", dev)
+        self.work = torch.zeros(_lib.NLB_DENSE_WORK_DOUBLES, dtype=torch.float64, device=dev)
         self.stream = torch.cuda.current_stream(dev)
         self.E = GpuEinsum(self.stream.cuda_stream)
         self.L = _lib.lib()
@@ -287,11 +350,10 @@ class DenseEngine:
         dev = self.dev
         r = [torch.zeros(s, dtype=torch.float64, device=dev)
              for s in ((p, h), (p, p), (p, p, h, h), (p, p), (p, p, h, h), (p, h, h, h), (p, h, h, h))]
-        if self.ppph[2]:
+        if self.ppph.nnz:
             ptrs = (ctypes.c_void_p * 7)(*[x.data_ptr() for x in r])
-            _lib.check(self.L.nlb_ppph_intermediates_f64(self.ppph[0].data_ptr(), self.ppph[1].data_ptr(),
-                                                         self.ppph[2], t1.data_ptr(), t2.data_ptr(), p, h, ptrs,
-                                                         self.sp), "ppph")
+            _lib.check(self.L.nlb_ppph_intermediates_f64(ctypes.byref(self.ppph.c), t1.data_ptr(), t2.data_ptr(),
+                                                         p, h, ptrs, self.sp), "ppph")
         ops = dict(T, t1=t1, t2=t2, r3=r[3], r4=r[4], r5=r[5], r6=r[6])
         # T1 equation (coupled_cluster.py:371-408)
         h1 = T["f_ph"].clone()
@@ -340,11 +402,11 @@ class DenseEngine:
                 self._term(n, ops, xhh2)
             for n in ("dgram_cdkl_bdkl", "dgram_cdlk_dk_bl"):
                 self._term(n, ops, xpp2)
-        if self.ppph[2]:
+        if self.ppph.nnz:
             _lib.check(self.L.nlb_antisym_acc_f64(r[2].data_ptr(), h2.data_ptr(), p, h, 2, 1.0, self.sp), "pij")
             for n in ("dgram_da_dbij", "dgram_acik_bcjk", "dgram_bijk_ak1", "dgram_bijk_ak2"):
                 self._term(n, ops, h2, tmp)
-        if self.pppp[2] or self.pppp_dense is not None:
+        if self.pppp.nnz or self.pppp_dense is not None:
             l1 = torch.zeros((p, p, h, h), dtype=torch.float64, device=dev)
             l2 = torch.zeros((p, p, h, h), dtype=torch.float64, device=dev)
             if self.pppp_dense is not None:
@@ -352,9 +414,8 @@ class DenseEngine:
                 self.E("abcd,cdij->abij", self.pppp_dense, t2, out=l1)
                 self.E("abcd,ci,dj->abij", self.pppp_dense, t1, t1, out=l2)
             else:
-                _lib.check(self.L.nlb_pppp_ladders_f64(self.pppp[0].data_ptr(), self.pppp[1].data_ptr(),
-                                                       self.pppp[2], t1.data_ptr(), t2.data_ptr(), p, h,
-                                                       l1.data_ptr(), l2.data_ptr(), self.sp), "pppp")
+                _lib.check(self.L.nlb_pppp_ladders_f64(ctypes.byref(self.pppp.c), t1.data_ptr(), t2.data_ptr(),
+                                                       p, h, l1.data_ptr(), l2.data_ptr(), self.sp), "pppp")
             _lib.check(self.L.nlb_antisym_acc_f64(l1.data_ptr(), h2.data_ptr(), p, h, 0, 0.5, self.sp), "l1")
             _lib.check(self.L.nlb_antisym_acc_f64(l2.data_ptr(), h2.data_ptr(), p, h, 2, 0.5, self.sp), "l2")
         self.E("bc,acij->abij", xpp2, t2, out=tmp)
@@ -369,7 +430,7 @@ class DenseEngine:
         v = self.T["v_pphh"] if self.nonzero["v_pphh"] else None
         _lib.check(self.L.nlb_dense_energy_f64(self.T["f_ph"].data_ptr(), t1.data_ptr(),
                                                v.data_ptr() if v is not None else None, t2.data_ptr(), self.p,
-                                               self.h, out.data_ptr(), self.sp), "energy")
+                                               self.h, out.data_ptr(), self.work.data_ptr(), self.sp), "energy")
 
 
 def solve(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5,
@@ -405,7 +466,7 @@ def solve(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_
     if use_diis:
         err = torch.zeros((max_diis, n1 + n2), dtype=torch.float64, device=dev)
         hist = torch.zeros((max_diis, n1 + n2), dtype=torch.float64, device=dev)
-        work = torch.zeros(512, dtype=torch.float64, device=dev)
+        work = torch.zeros(_lib.NLB_DENSE_WORK_DOUBLES, dtype=torch.float64, device=dev)
         nerr = 0
     e_buf = torch.zeros(1, dtype=torch.float64, device=dev)
     eng.energy(t1, t2, e_buf)

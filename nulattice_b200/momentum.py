@@ -263,7 +263,7 @@ def solve(plan, V, fpp, fhh, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mi
     if use_diis:
         err = torch.zeros((max_diis, n), dtype=torch.float64, device=eng.dev)
         hist = torch.zeros((max_diis, n), dtype=torch.float64, device=eng.dev)
-        work = torch.zeros(512, dtype=torch.float64, device=eng.dev)
+        work = torch.zeros(_lib.NLB_DENSE_WORK_DOUBLES, dtype=torch.float64, device=eng.dev)
         nerr = 0
     prev = float(eng.energy(xs[cur]).item())
     if verbose:

@@ -1,9 +1,9 @@
 """Generate the golden vectors that pin the CCSD oracle to the reference.
 
-Run in a container where the reference NuLattice tree is mounted read-only
-(default ``/root/reference``; override with ``NULATTICE_REF``):
+Run where a checkout of the reference NuLattice tree is available, with
+``NULATTICE_REF`` naming its root (the directory holding ``src/NuLattice``):
 
-    python tests/golden/make_goldens.py [case ...]
+    NULATTICE_REF=<reference root> python tests/golden/make_goldens.py [case ...]
 
 Everything here calls the reference's own code (``CCM/coupled_cluster.py``,
 ``CCM/ccDgrams.py``, ``CCM/soa/coupled_cluster.py``, ``lattice.py``) and
@@ -20,7 +20,9 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("NULATTICE_REF", "/root/reference")
+REF = os.environ.get("NULATTICE_REF")
+if not REF or not os.path.isdir(os.path.join(REF, "src", "NuLattice")):
+    sys.exit("set NULATTICE_REF to the root of a NuLattice checkout (the directory holding src/NuLattice)")
 sys.path.insert(0, os.path.join(HERE, "_standin"))
 sys.path.insert(0, os.path.join(REF, "src"))
 
@@ -295,6 +297,7 @@ CASES = {
     "he4_L4_c2": lambda: case_system("he4_L4_c2", 4, "he4", -6.0, 2.0, store_t2=False),
     "a28_L4": lambda: case_system("a28_L4", 4, "a28", -6.0, 2.0, tight=False, store_t2=False,
                                   traj_steps=2),
+    "he4_L5_c3": lambda: case_system("he4_L5_c3", 5, "he4", -6.0, 2.0, store_t2=False, eps=1e-13),
     "a28_L4_tight": lambda: case_system("a28_L4_tight", 4, "a28", -6.0, 2.0, store_t2=False,
                                         traj_steps=1, eps=1e-13),
     "soa_diis": case_soa_diis,
