@@ -22,7 +22,7 @@ def _solve(tag, **kw):
     return g, out, info
 
 
-@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he4_L4_c2"])
+@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he4_L4_c2", "he4_L5_c3"])
 def test_tight_energy_matches_reference(tag):
     """Fixed point of the reference's own NumPy solver, 1e-10 relative."""
     g, (e, t1, t2), info = _solve(tag, eps=float(g_eps(tag)), maxSteps=5000, max_diis=0,
@@ -38,7 +38,7 @@ def g_eps(tag):
     return float(G.load(tag)["tight_eps"])
 
 
-@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he4_L4_c2"])
+@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he4_L4_c2", "he4_L5_c3"])
 def test_trajectory_matches_reference(tag):
     g = G.load(tag)
     _, (e, t1, t2), info = _solve(tag, eps=0.0, maxSteps=int(g["traj_steps"]), max_diis=0,
@@ -86,7 +86,7 @@ def test_a28_two_steps_match_reference():
     assert np.linalg.norm(t2) == pytest.approx(float(g["traj_t2_norm"]), rel=1e-11)
 
 
-@pytest.mark.parametrize("tag", ["he4_L3_c1", "he4_L4_c2"])
+@pytest.mark.parametrize("tag", ["he4_L3_c1", "he4_L4_c2", "he4_L5_c3"])
 def test_mixed_precision_energy(tag):
     g = G.load(tag)
     ref = float(g["tight_e"])
