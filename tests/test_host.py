@@ -204,7 +204,8 @@ def test_dense_blocks_are_row_major_whatever_the_input_strides():
 
 PAIRS = [("StructProblem", "nlb_struct_problem"), ("Ctrl", "nlb_ctrl"), ("StructState", "nlb_struct_state"),
          ("LambdaState", "nlb_lambda_state"), ("BatchItem", "nlb_batch_item"), ("BatchConfig", "nlb_batch_config"),
-         ("ContractDesc", "nlb_contract_desc"), ("PwProblem", "nlb_pw_problem"), ("PwState", "nlb_pw_state")]
+         ("ContractDesc", "nlb_contract_desc"), ("PwProblem", "nlb_pw_problem"), ("PwState", "nlb_pw_state"),
+         ("PpphPlan", "nlb_ppph_plan"), ("PpppPlan", "nlb_pppp_plan")]
 
 
 def test_ctypes_mirrors_match_the_c_header(tmp_path):
@@ -236,3 +237,14 @@ def test_ctypes_mirrors_match_the_c_header(tmp_path):
     assert len(got) == len(want)
     bad = [(w, g) for w, g in zip(want, got) if w[2] != g]
     assert not bad, bad
+
+
+def test_dense_work_size_matches_the_header():
+    """The ctypes constant sizing the dense engine's work buffers equals the
+    header's NLB_DENSE_WORK_DOUBLES."""
+    import os
+    import re
+    from nulattice_b200 import _lib
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "nulattice_b200.h")).read()
+    assert int(re.search(r"#define NLB_DENSE_WORK_DOUBLES (\d+)", hdr).group(1)) == _lib.NLB_DENSE_WORK_DOUBLES
