@@ -340,6 +340,22 @@ int64_t nlb_contract_gemm_work(const nlb_contract_desc *d);
 int nlb_contract_gemm_f64(const nlb_contract_desc *d, const double *A, const double *B, double *C,
                           double alpha, double beta, double *work, int64_t work_bytes, nlb_stream_t stream);
 
+/* The same contraction on the tensor cores (mixed-precision phase of the
+ * general engine): the operands are split into TF32 parts, A ~ A_hi + A_lo,
+ * B ~ B_hi + B_lo, and C ~ alpha (A_hi B_hi + A_hi B_lo + A_lo B_hi) + beta C
+ * with FP32 accumulation in tensor memory (tcgen05.mma kind::tf32, 128x128
+ * tiles, TMA-staged operands, split-K when the tiles are fewer than the SMs;
+ * the split partials are added in a fixed order).  Relative accuracy is that
+ * of FP32 (about 1e-6 of the largest product).  `work` holds
+ * nlb_contract_gemm_tc_work(d) bytes and starts on a 256-byte boundary.  A
+ * tile whose bounded waits ran out turns every output entry into NaN.
+ * Replaces, in the mixed phase, the library GEMM that evaluates the ring,
+ * quadratic and dense-ladder diagrams (ccDgrams.py:253-303, 359-385,
+ * 474-500). */
+int64_t nlb_contract_gemm_tc_work(const nlb_contract_desc *d);
+int nlb_contract_gemm_tf32x3(const nlb_contract_desc *d, const double *A, const double *B, double *C,
+                             double alpha, double beta, void *work, int64_t work_bytes, nlb_stream_t stream);
+
 /* H += alpha * P(Z) on (p,p,h,h) tensors, P = 1, pAB, pIJ or pIJ pAB
  * (perm 0..3; ccDgrams.py:193-213). */
 int nlb_antisym_acc_f64(const double *Z, double *H, int64_t p, int64_t h, int32_t perm,

@@ -164,6 +164,11 @@ def lib():
     L.nlb_contract_gemm_work.restype = c_int64
     L.nlb_contract_gemm_f64.argtypes = [ctypes.POINTER(ContractDesc), c_void_p, c_void_p, c_void_p, c_double,
                                         c_double, c_void_p, c_int64, c_void_p]
+    L.nlb_contract_gemm_tc_work.argtypes = [ctypes.POINTER(ContractDesc)]
+    L.nlb_contract_gemm_tc_work.restype = c_int64
+    L.nlb_contract_gemm_tf32x3.argtypes = [ctypes.POINTER(ContractDesc), c_void_p, c_void_p, c_void_p, c_double,
+                                           c_double, c_void_p, c_int64, c_void_p]
+    L.nlb_contract_gemm_tf32x3.restype = c_int32
     L.nlb_antisym_acc_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int64, c_int32, c_double, c_void_p]
     L.nlb_ppph_intermediates_f64.argtypes = [ctypes.POINTER(PpphPlan), c_void_p, c_void_p, c_int64, c_int64,
                                              c_void_p, c_void_p]

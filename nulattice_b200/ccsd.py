@@ -21,7 +21,9 @@ Extra keyword-only arguments (not in the reference):
 ``precision``  ``"fp64"`` (default) or ``"mixed"`` -- the structured engine
                stores T2 in FP32 and computes the elementwise work in FP32
                (T1, energies, norms and DIIS stay FP64), then finishes with
-               FP64 steps until ``eps`` is met.
+               FP64 steps until ``eps`` is met; the general engine runs its
+               GEMM-shaped contractions on the tensor cores (3xTF32, FP32
+               accumulation) until ``mixed_eps``, then in FP64 to ``eps``.
 ``criterion``  ``"soa"`` (default: ``|dE|/max(1,|E|) < eps`` and pulsed DIIS,
                as the torch solver) or ``"numpy"`` (``|dE|/|E| < eps``, no
                DIIS, as the NumPy solver whose DIIS branch never fires).
@@ -463,7 +465,8 @@ def ccsd_solver(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000
         info["why_general"] = why
         e, t1, t2 = _dense.solve(fock_mats, two_body_int, t1initial=t1initial, eps=eps, maxSteps=maxSteps,
                                  max_diis=max_diis, delta=delta, mixing=mixing, verbose=verbose, ccs=ccs,
-                                 device=dev, criterion=criterion, info=info)
+                                 device=dev, criterion=criterion, info=info, precision=precision,
+                                 mixed_eps=mixed_eps)
     else:
         info["engine"] = "structured"
         t0 = time.perf_counter()

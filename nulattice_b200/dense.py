@@ -79,8 +79,11 @@ TERMS = {
 DENSE_PPPP_FRACTION = 8
 
 # contractions with at least this many multiply-adds (and no batch index)
-# go through gathered panels and one library GEMM (FP64 tensor cores)
+# go through gathered panels and one GEMM: the FP64 library GEMM, or in the
+# mixed phase the 3xTF32 tcgen05 kernel when both GEMM sides have at least
+# TC_MIN_MN rows (its tiles are 128 x 128)
 GEMM_MIN_MACS = 1 << 18
+TC_MIN_MN = 32
 
 
 class GpuEinsum:
@@ -94,6 +97,13 @@ class GpuEinsum:
         self._ws = None
         self.launches = 0
         self.gemms = 0
+        self.tc_gemms = 0
+        self.tensor_cores = False    # mixed phase: GEMM-shaped contractions on the tcgen05 kernel
+
+    def _workspace(self, nbytes, device):
+        if self._ws is None or self._ws.numel() * 8 < nbytes:
+            self._ws = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=device)
+        return self._ws
 
     # -- one pairwise contraction ------------------------------------------
     def pair(self, spec, A, B, out, alpha=1.0, beta=0.0):
@@ -139,10 +149,17 @@ class GpuEinsum:
         prod = lambda g: int(np.prod([ext[x] for x in groups[g]])) if groups[g] else 1  # noqa: E731
         d.M, d.N, d.K, d.B = prod("m"), prod("n"), prod("k"), prod("b")
         if d.B == 1 and d.K > 0 and d.M * d.N * d.K >= GEMM_MIN_MACS:
+            if self.tensor_cores and min(d.M, d.N) >= TC_MIN_MN:
+                ws = self._workspace(int(self.L.nlb_contract_gemm_tc_work(ctypes.byref(d))), out.device)
+                _lib.check(self.L.nlb_contract_gemm_tf32x3(ctypes.byref(d), A.data_ptr(), B.data_ptr(),
+                                                           out.data_ptr(), alpha, beta, ws.data_ptr(),
+                                                           ws.numel() * 8, self.sp), "contract (tensor cores)")
+                self.launches += 4
+                self.tc_gemms += 1
+                return
             # large contractions: gathered panels and one library GEMM
             need = int(self.L.nlb_contract_gemm_work(ctypes.byref(d)))
-            if self._ws is None or self._ws.numel() * 8 < need:
-                self._ws = torch.empty((need + 7) // 8, dtype=torch.float64, device=out.device)
+            self._workspace(need, out.device)
             _lib.check(self.L.nlb_contract_gemm_f64(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
                                                     alpha, beta, self._ws.data_ptr(), self._ws.numel() * 8,
                                                     self.sp), "contract (gemm)")
@@ -434,13 +451,20 @@ class DenseEngine:
 
 
 def solve(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5,
-          verbose=False, ccs=False, device=None, criterion="soa", info=None):
+          verbose=False, ccs=False, device=None, criterion="soa", info=None, precision="fp64", mixed_eps=None):
     """The solver loop of ``CCM/soa/coupled_cluster.py:440-575`` (criterion
     ``"soa"``) or ``CCM/coupled_cluster.py:547-687`` (``"numpy"``) on the
-    dense GPU engine.  Returns ``(E_corr, t1, t2)`` as CUDA tensors."""
+    dense GPU engine.  Returns ``(E_corr, t1, t2)`` as CUDA tensors.
+
+    ``precision="mixed"``: the GEMM-shaped contractions run on the tensor
+    cores (3xTF32) until the energy test passes at ``mixed_eps``; the solve
+    then continues from those amplitudes with FP64 contractions to ``eps``."""
     info = {} if info is None else info
     t0 = time.perf_counter()
     eng = DenseEngine(fock_mats, two_body_int, device)
+    mixed = precision == "mixed"
+    tol = (float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)) if mixed else float(eps)
+    eng.E.tensor_cores = mixed
     L, sp, dev = eng.L, eng.sp, device
     p, h = eng.p, eng.h
     n1, n2 = p * h, p * p * h * h
@@ -497,9 +521,16 @@ def solve(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_
         if verbose:
             print(f"Step {it}: {e}", "difference =", abs(e - prev) / abs(e) if e != 0 else float("inf"))
         if criterion == "soa":
-            done = abs(e - prev) / max(1.0, abs(e)) < eps
+            done = abs(e - prev) / max(1.0, abs(e)) < tol
         else:
-            done = (e == 0 and prev == 0) or (e != 0 and abs(e - prev) / abs(e) < eps)
+            done = (e == 0 and prev == 0) or (e != 0 and abs(e - prev) / abs(e) < tol)
+        if done and eng.E.tensor_cores:
+            # end of the tensor-core phase: FP64 contractions from here on
+            eng.E.tensor_cores = False
+            info["mixed_iters"] = it
+            info["mixed_energy"] = e
+            tol = float(eps)
+            done = False
         if done:
             status = "converged"
             break
@@ -516,6 +547,6 @@ def solve(fock_mats, two_body_int, t1initial=None, eps=1e-8, maxSteps=1000, max_
         prev = e
     torch.cuda.current_stream(dev).synchronize()
     info.update(status=status, iterations=it, t_iterate=time.perf_counter() - t0,
-                launches=eng.E.launches)
+                launches=eng.E.launches, tc_gemms=eng.E.tc_gemms, gemms=eng.E.gemms)
     t1, t2 = views(xs[cur])
     return e, t1.clone(), t2.clone()
