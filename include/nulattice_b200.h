@@ -235,7 +235,7 @@ typedef struct {
     const void *t2;     /* converged compact t2 [n_t2] (dtype) */
     double *prep;       /* [nlb_struct_prep_len] tables at the converged t1 (filled by init) */
     void *ga;           /* [n_g] Ga of the converged t2 (dtype, filled by init) */
-    void *ha;           /* [n_g] scratch (dtype) */
+    void *ha;           /* [nlb_lambda_ha_len] scratch (dtype) */
     double *acc;        /* [nlb_lambda_acc_len] scratch; after a step it holds Y1, U, T */
     nlb_ctrl *ctrl;
     void *gb;           /* [nlb_lambda_gb_len] Gb of every row of the converged t2 (dtype, lattice path) */
@@ -248,6 +248,10 @@ typedef struct {
 #define NLB_LAMBDA_KEEP 1   /* nlb_lambda_init: start from lam1[0], lam2[0] instead of zero */
 
 int64_t nlb_lambda_acc_len(const nlb_struct_problem *prob);
+/* Length (elements of the state's dtype) of the `ha` scratch: on the lattice
+ * path one slice of n_g per row chunk of the column pass (each slice has one
+ * writer per element; the slices are added in chunk order), else n_g. */
+int64_t nlb_lambda_ha_len(const nlb_struct_problem *prob);
 int64_t nlb_lambda_gb_len(const nlb_struct_problem *prob);
 /* 1 when the lattice path applies to prob (FP32 and DIIS available). */
 int32_t nlb_lambda_lattice(const nlb_struct_problem *prob);

@@ -179,6 +179,8 @@ def lib():
                                        c_void_p, c_void_p]
     L.nlb_lambda_acc_len.argtypes = [ctypes.POINTER(StructProblem)]
     L.nlb_lambda_acc_len.restype = c_int64
+    L.nlb_lambda_ha_len.argtypes = [ctypes.POINTER(StructProblem)]
+    L.nlb_lambda_ha_len.restype = c_int64
     L.nlb_lambda_gb_len.argtypes = [ctypes.POINTER(StructProblem)]
     L.nlb_lambda_gb_len.restype = c_int64
     L.nlb_lambda_lattice.argtypes = [ctypes.POINTER(StructProblem)]

@@ -98,7 +98,7 @@ class LambdaSolver:
             t2=torch.zeros(max(pl.n_t2, 1), **ft),
             prep=torch.zeros(int(L.nlb_struct_prep_len(eng.prob)), **f64),
             ga=torch.zeros(max(eng.n_g, 1), **ft),
-            ha=torch.zeros(max(eng.n_g, 1), **ft),
+            ha=torch.zeros(max(int(L.nlb_lambda_ha_len(eng.prob)), 1), **ft),
             gb=torch.zeros(max(self.n_gb, 1), **ft),
             acc=torch.zeros(int(L.nlb_lambda_acc_len(eng.prob)), **f64),
             ctrl=torch.zeros(ctypes.sizeof(_lib.Ctrl), dtype=torch.uint8, device=dev),

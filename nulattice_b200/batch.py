@@ -164,7 +164,8 @@ class _Instance:
                      lam2=[torch.zeros(n2, **ft) for _ in range(2)],
                      t2=torch.zeros(n2, **ft) if own_t2 else None,
                      prep=torch.zeros(prep_len, **f64), ga=torch.zeros(max(eng.n_g, 1), **ft),
-                     ha=torch.zeros(max(eng.n_g, 1), **ft), gb=torch.zeros(max(n_gb, 1), **ft),
+                     ha=torch.zeros(max(int(L_.nlb_lambda_ha_len(eng.prob)), 1), **ft),
+                     gb=torch.zeros(max(n_gb, 1), **ft),
                      acc=torch.zeros(acc_len, **f64),
                      ctrl=torch.zeros(ctypes_sizeof_ctrl(), dtype=torch.uint8, device=dev))
             return b

@@ -53,10 +53,26 @@ int lcheck(const char* where) {
     return NLB_OK;
 }
 
-// scratch layout (doubles): Y1[p*h] Z1 contributions gathered from T2 rows,
-// U[h*h] = t1^T lam1, T[h*h] X_hh contractions, fc[n_t1c] f_ph per label.
+// scratch layout (doubles): Y1[p*h] Z1 contributions gathered from T2 rows
+// (general path), U[h*h] = t1^T lam1, T[h*h] X_hh contractions, fc[n_t1c]
+// f_ph per label, and the lattice path's per-writer slots: Y1r[n_f2] (the Z1
+// contribution of row a' of each channel, [a'][k']), Y1c[kMaxColChunks][n_f2]
+// (of column b' and one row chunk of the column pass, [b'][k']) and
+// Tp[col items][2][49] (the X_hh contractions of one column-pass block, g1
+// side then g2 side).  Every slot has exactly one writer; k_l_t1 and
+// k_l_treduce add them in a fixed order, so the lattice path's Lambda solve
+// repeats bit for bit.
+constexpr int kMaxColChunks = 8;       // row chunks of the column pass
+constexpr int kLHP_ = 49;              // hole pairs per channel block on the lattice path
+constexpr int kColNB = 256 / kLHP_;    // column-pass b' per block (kColThreads / 49)
+
+__host__ __device__ inline int64_t col_items_max(const nlb_struct_problem& P) {
+    const int64_t np = P.max_row / kLHP_;
+    return (int64_t)P.n_channels * ((np + kColNB - 1) / kColNB) * kMaxColChunks;
+}
+
 struct LView {
-    double *Y1, *U, *T, *fc;
+    double *Y1, *U, *T, *fc, *Y1r, *Y1c, *Tp;
 };
 
 __host__ __device__ inline LView lview(double* acc, const nlb_struct_problem& P) {
@@ -65,6 +81,9 @@ __host__ __device__ inline LView lview(double* acc, const nlb_struct_problem& P)
     v.U = v.Y1 + (int64_t)P.p * P.h;
     v.T = v.U + (int64_t)P.h * P.h;
     v.fc = v.T + (int64_t)P.h * P.h;
+    v.Y1r = v.fc + P.n_t1c;
+    v.Y1c = v.Y1r + P.n_f2;
+    v.Tp = v.Y1c + (int64_t)kMaxColChunks * P.n_f2;
     return v;
 }
 
@@ -307,8 +326,10 @@ __global__ void k_l_u(nlb_struct_problem P, nlb_lambda_state S) {
     }
 }
 
-// Z1 and the Jacobi update of lam1.
-__global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
+// Z1 and the Jacobi update of lam1.  nchunk > 0 (lattice path): the Z1
+// contributions come from the row and column slots (Y1r, Y1c), added in
+// channel order; 0 (general path): from the Y1 accumulator.
+__global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S, int nchunk) {
     nlb_ctrl* c = S.ctrl;
     if (c->status != NLB_RUNNING) return;
     const int par = c->parity;
@@ -330,7 +351,20 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S) {
             if (E1) E1[idx] = 0.0;
             continue;
         }
-        double Z = P.f_ph[idx] + V.Y1[idx];
+        double y1 = 0.0;
+        if (nchunk > 0) {
+            const int xl = P.p_loc[x], ml = P.h_loc[mm];
+            for (int ci = 0; ci < P.n_channels; ++ci) {
+                const nlb_channel& ch = P.chan[ci];
+                const int64_t o = ch.f2_off + (int64_t)xl * ch.nh1 + ml;
+                if (ch.g1 == g) y1 += V.Y1r[o];
+                if (ch.g2 == g)
+                    for (int cq = 0; cq < nchunk; ++cq) y1 += V.Y1c[(int64_t)cq * P.n_f2 + o];
+            }
+        } else {
+            y1 = V.Y1[idx];
+        }
+        double Z = P.f_ph[idx] + y1;
         const int pb = P.p_base[g];
         const int r = pb + P.p_loc[x];
         for (int q = P.fpp_ptr[r]; q < P.fpp_ptr[r + 1]; ++q)
@@ -605,11 +639,14 @@ __global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lamb
             }
             row(r, x0, bc0, br0, g0);
         }
+        // this chunk's slice of Ha (one writer per element: no zeroing, no atomics)
+        T* hc = ha + (int64_t)chunk * P.n_g + ch.ga_off;
 #pragma unroll
-        for (int k = 0; k < kLH; ++k) atomicAdd(&ha[ch.ga_off + (int64_t)k * rowlen + col], hak[k]);
+        for (int k = 0; k < kLH; ++k) hc[(int64_t)k * rowlen + col] = hak[k];
     }
-    const int h = P.h;
-    // Y1[b', k'] = sum over the group's hole pairs of -ys[k'] + (k' == j') ylt
+    // Y1[b', k'] of this chunk = sum over the group's hole pairs of -ys[k'] +
+    // (k' == j') ylt, into the chunk's slot (the lattice path's uniform
+    // channels give the column side the [b'][k'] layout of F2)
 #pragma unroll
     for (int k = 0; k < kLH; ++k) sv[tid][k] = act ? (double)(-ys[k]) + (k == jp ? (double)ylt : 0.0) : 0.0;
     __syncthreads();
@@ -619,11 +656,13 @@ __global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lamb
         if (b2 < ch.np2) {
             double s = 0.0;
             for (int q = 0; q < kLHP; ++q) s += sv[g2 * kLHP + q][k];
-            atomicAdd(&V.Y1[(int64_t)P.p_ord[ch.pb2 + b2] * h + P.h_ord[ch.hb2 + k]], s);
+            V.Y1c[(int64_t)chunk * P.n_f2 + ch.f2_off + (int64_t)b2 * kLH + k] = s;
         }
     }
     __syncthreads();
-    // T[k', i'] (g1) = sum over threads with that i'; then T[k', j'] (g2) likewise
+    // T[k', i'] (g1) = sum over threads with that i'; then T[k', j'] (g2)
+    // likewise, into this block's slot (k_l_treduce adds the blocks)
+    double* tp = V.Tp + (int64_t)blockIdx.x * 2 * kLHP;
     for (int side = 0; side < 2; ++side) {
 #pragma unroll
         for (int k = 0; k < kLH; ++k) sv[tid][k] = act ? (double)(side ? tt2[k] : tt1[k]) : 0.0;
@@ -633,10 +672,59 @@ __global__ void __launch_bounds__(NT, 2) k_l_cols(nlb_struct_problem P, nlb_lamb
             double s = 0.0;
             for (int g2 = 0; g2 < NB; ++g2)
                 for (int o = 0; o < kLH; ++o) s += sv[g2 * kLHP + (side ? o * kLH + i : i * kLH + o)][k];
-            const int hb = side ? ch.hb2 : ch.hb1;
-            atomicAdd(&V.T[(int64_t)P.h_ord[hb + k] * h + P.h_ord[hb + i]], s);
+            tp[side * kLHP + w] = s;
         }
         __syncthreads();
+    }
+}
+
+// The column pass's slots, added in a fixed order.  Blocks 0 ..
+// n_labels * 49 - 1: T[k, m] for one (label g, local holes k', i'); the
+// threads take the column-pass blocks strided (their g1 side and g2 side
+// values), the block tree adds them.  The remaining blocks add the Ha chunk
+// slices into slice 0, element by element in chunk order, for the row pass.
+__global__ void k_l_treduce(nlb_struct_problem P, nlb_lambda_state S, int nchunk, int n_items, int elsize) {
+    const nlb_ctrl* c = S.ctrl;
+    if (c->status != NLB_RUNNING) return;
+    const LView V = lview(S.acc, P);
+    const int nt_out = P.n_labels * kLHP;
+    if ((int)blockIdx.x < nt_out) {
+        const int g = blockIdx.x / kLHP, w = blockIdx.x - g * kLHP;
+        double s = 0.0;
+        for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
+            // the channel of column-pass block `it` (numbered channel by channel)
+            int64_t item0 = 0;
+            int ci = 0;
+            for (; ci < P.n_channels - 1; ++ci) {
+                const int64_t nit = (int64_t)((P.chan[ci].np2 + kColNB - 1) / kColNB) * nchunk;
+                if (it < item0 + nit) break;
+                item0 += nit;
+            }
+            const nlb_channel& ch = P.chan[ci];
+            if (ch.g1 == g) s += V.Tp[(int64_t)it * 2 * kLHP + w];
+            if (ch.g2 == g) s += V.Tp[(int64_t)it * 2 * kLHP + kLHP + w];
+        }
+        s = block_sum(s);
+        if (threadIdx.x == 0) {
+            const int hb = P.h_base[g];
+            V.T[(int64_t)P.h_ord[hb + w / kLH] * P.h + P.h_ord[hb + w % kLH]] = s;
+        }
+        return;
+    }
+    if (nchunk < 2) return;
+    const int64_t nb = (int64_t)gridDim.x - nt_out;
+    for (int64_t e = ((int64_t)blockIdx.x - nt_out) * blockDim.x + threadIdx.x; e < P.n_g; e += nb * blockDim.x) {
+        if (elsize == 4) {
+            float* ha = static_cast<float*>(S.ha);
+            float v = ha[e];
+            for (int cq = 1; cq < nchunk; ++cq) v += ha[(int64_t)cq * P.n_g + e];
+            ha[e] = v;
+        } else {
+            double* ha = static_cast<double*>(S.ha);
+            double v = ha[e];
+            for (int cq = 1; cq < nchunk; ++cq) v += ha[(int64_t)cq * P.n_g + e];
+            ha[e] = v;
+        }
     }
 }
 
@@ -900,7 +988,7 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
         if (tid < kLH) {
             double s = 0.0;
             for (int w = 0; w < NT / 32; ++w) s += sred[w][tid];
-            atomicAdd(&V.Y1[(int64_t)a * h + P.h_ord[ch.hb1 + tid]], s);
+            V.Y1r[ch.f2_off + (int64_t)ap * kLH + tid] = s;   // this block owns row a' of the channel
         }
         __syncthreads();
     }
@@ -951,6 +1039,11 @@ constexpr int kColThreads = 256;
 
 bool lattice(const nlb_struct_problem* P) {
     if (P->uniform_nh != kLH || !P->diag_ladders || P->max_fpp_offdiag > kLNa || P->n_t2 <= 0) return false;
+    // every channel np1 = np2 = max_row / 49 (the column-side slots share the
+    // row side's [particle][hole] layout): the row count and the amplitude
+    // count reach their maxima only then
+    const int64_t np = P->max_row / kLHP;
+    if (P->n_rows != (int64_t)P->n_channels * np || P->n_t2 != (int64_t)P->n_channels * np * np * kLHP) return false;
     return llat_smem(P->max_row, kLatThreads / kLHP, 8).total + 1024 <= optin_smem();
 }
 
@@ -1011,19 +1104,24 @@ int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_
     constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
     const int64_t hh = (int64_t)P->h * P->h;
     k_l_u<<<grid_l(32 * hh + (int64_t)P->p * P->h), kThreads, 0, s>>>(*P, *S);
-    cudaMemsetAsync(S->ha, 0, sizeof(T) * (size_t)P->n_g, s);
+    // every label has the same particle count on the lattice path; row
+    // chunks from the tuning word (bits 8-15, 0: automatic), at most
+    // kMaxColChunks (the slots of the column pass)
+    constexpr int NB = kColThreads / kLHP;
+    static_assert(NB == kColNB, "column-pass blocks");
+    const int tuned = (P->tune >> 8) & 255;
+    const int64_t np1 = P->max_row / kLHP;
+    int nchunk = tuned > 0 ? (int)(tuned < np1 ? tuned : np1) : col_chunks(P);
+    const int need = (int)((np1 + kColRows - 1) / kColRows);   // rows of a chunk fit the staging
+    if (nchunk < need) nchunk = need;
+    if (nchunk > kMaxColChunks) nchunk = kMaxColChunks;
+    if (nchunk < need) return lfail(NLB_ERR_SIZE, "nlb_lambda_step: rows too long for the column pass");
     {
-        // every label has the same particle count on the lattice path;
-        // row chunks from the tuning word (bits 8-15, 0: automatic)
-        constexpr int NB = kColThreads / kLHP;
-        const int tuned = (P->tune >> 8) & 255;
-        const int64_t np1 = P->max_row / kLHP;
-        int nchunk = tuned > 0 ? (int)(tuned < np1 ? tuned : np1) : col_chunks(P);
-        const int need = (int)((np1 + kColRows - 1) / kColRows);   // rows of a chunk fit the staging
-        if (nchunk < need) nchunk = need;
         const int64_t np2 = P->max_row / kLHP;
         const int64_t items = (np2 + NB - 1) / NB * nchunk * P->n_channels;
         k_l_cols<T, kColThreads><<<(unsigned)items, kColThreads, 0, s>>>(*P, *S, nchunk);
+        const int hblocks = nchunk > 1 ? grid_l(P->n_g) : 0;
+        k_l_treduce<<<P->n_labels * kLHP + hblocks, 128, 0, s>>>(*P, *S, nchunk, (int)items, (int)sizeof(T));
     }
     // row-pass launch shape from the tuning word (bits 4-7)
     int n2 = 0;
@@ -1035,7 +1133,7 @@ int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_
     }
     if (cudaPeekAtLastError() != cudaSuccess) return lcheck("nlb_lambda_step");
     const int n1 = grid_l((int64_t)P->p * P->h);
-    k_l_t1<<<n1, kThreads, 0, s>>>(*P, *S);
+    k_l_t1<<<n1, kThreads, 0, s>>>(*P, *S, nchunk);
     k_l_finish<<<1, 32, 0, s>>>(S->ctrl, prep_view(S->prep, *P).red, n1, n2);
     return lcheck("nlb_lambda_step");
 }
@@ -1046,7 +1144,13 @@ extern "C" {
 
 int64_t nlb_lambda_acc_len(const nlb_struct_problem* prob) {
     if (!prob) return 0;
-    return (int64_t)prob->p * prob->h + 2 * (int64_t)prob->h * prob->h + prob->n_t1c;
+    return (int64_t)prob->p * prob->h + 2 * (int64_t)prob->h * prob->h + prob->n_t1c +
+           (int64_t)(1 + kMaxColChunks) * prob->n_f2 + col_items_max(*prob) * 2 * kLHP;
+}
+
+int64_t nlb_lambda_ha_len(const nlb_struct_problem* prob) {
+    if (!prob) return 0;
+    return lattice(prob) ? (int64_t)kMaxColChunks * prob->n_g : prob->n_g;
 }
 
 int64_t nlb_lambda_gb_len(const nlb_struct_problem* prob) {
@@ -1112,7 +1216,7 @@ int nlb_lambda_step(const nlb_struct_problem* prob, const nlb_lambda_state* st, 
     if (grid < 1) grid = 1;
     k_l_rows<<<(unsigned)grid, kThreads, (size_t)sm, s>>>(*prob, *st);
     const int n1 = grid_l((int64_t)prob->p * prob->h);
-    k_l_t1<<<n1, kThreads, 0, s>>>(*prob, *st);
+    k_l_t1<<<n1, kThreads, 0, s>>>(*prob, *st, 0);
     k_l_finish<<<1, 32, 0, s>>>(st->ctrl, prep_view(st->prep, *prob).red, n1, (int)grid);
     return lcheck("nlb_lambda_step");
 }

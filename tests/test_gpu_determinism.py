@@ -63,3 +63,20 @@ def test_momentum_engine_repeats():
     assert i0["status"] == "converged" and i0["iterations"] == i1["iterations"]
     assert r0[0] == r1[0]
     assert torch.equal(r0[2], r1[2])
+
+
+def test_lambda_lattice_path_repeats():
+    """The coupling derivatives through the lattice Lambda kernels: the Z1
+    contributions, Ha and the X_hh contractions sit in per-writer slots that
+    are added in a fixed order, so two gradient solves agree bit for bit."""
+    from nulattice_b200 import adjoint as A
+    holes = ham.closed_shell_holes(4, 28)
+    runs = []
+    for _ in range(2):
+        info = {}
+        E, g2, g3 = A.ccsd_energy_and_gradient(4, holes, -3.0, 1.0, device=DEV, precision="mixed", eps=1e-10,
+                                               mixed_eps=1e-8, lambda_tol=1e-9, info=info)
+        torch.cuda.synchronize()
+        runs.append((E, g2, g3, info["lambda_iters"], info.get("lambda_path")))
+    assert runs[0][4] == "lattice"
+    assert runs[0] == runs[1]
