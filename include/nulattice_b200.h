@@ -67,7 +67,8 @@ typedef struct {
     int32_t max_fpp_offdiag;      /* most off-diagonal entries in one f_pp row */
     int32_t tune;                 /* launch shapes, 0 = defaults (threads x resident blocks/SM):
                                      bits 0-3 lattice T2 kernel, FP32 (0 256x2, 1 512x1, 2 384x1;
-                                       packed FP32x2 sums: 3 512x1, 4 384x1);
+                                       packed FP32x2 sums: 3 512x1, 4 384x1; two rows per
+                                       pass: 5 256x1, 6 384x1, 7 448x1, 8 512x1);
                                      bits 4-7 lattice Lambda row pass, FP32 (0 256x2, 1 512x1);
                                      bits 8-15 Lambda column-pass row chunks (0: automatic);
                                      bits 16-19 lattice T2 kernel, FP64 (0 512x1, 1 256x1) */

@@ -713,6 +713,8 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
     if (threadIdx.x == 0) V.slots(kRedDt2)[blockIdx.x] = 4.0 * s;
 }
 
+#include "t2_pair.cuh"
+
 // --------------------------------------------------------- T1 update ----
 // R1 = f_ph + F2 + f_pp t1 - t1 Q/2 + t1 X_hh(T1 eq); Jacobi + mixing;
 // energy sum_ai f_ai t1'_ai (coupled_cluster.py:342-414, 265-286).
@@ -1285,6 +1287,19 @@ int64_t launch_lat(const nlb_struct_problem* P, const nlb_struct_state* S, cudaS
     return grid;
 }
 
+// The two-row lattice T2 kernel (FP32) with NT threads per block; falls
+// back to the one-row kernel when two double-buffered row pairs do not fit
+// in shared memory.
+template <int NT, int MINB>
+int64_t launch_pair(const nlb_struct_problem* P, const nlb_struct_state* S, cudaStream_t st, bool launch = true) {
+    const int64_t sm = pair_smem(P->max_row).total;
+    if (sm + 1024 > smem_limit()) return launch_lat<float, 512, 1, true>(P, S, st, launch);
+    auto kern = k_t2_pair<NT, MINB>;
+    const int64_t grid = reducing_grid(blocks_per_sm(reinterpret_cast<const void*>(kern), sm, NT), P->n_rows);
+    if (launch) kern<<<(unsigned)grid, NT, (size_t)sm, st>>>(*P, *S);
+    return grid;
+}
+
 // The T2 update of one step (lattice or general kernel); returns its grid,
 // 0 when there is no T2.  launch = false only computes the grid.
 template <typename T>
@@ -1295,6 +1310,10 @@ int64_t t2_update(const nlb_struct_problem* P, const nlb_struct_state* S, cudaSt
         // bits 16-19), see nlb_struct_problem
         if constexpr (sizeof(T) == 4) {
             const int v = P->tune & 15;
+            if (v == 5) return launch_pair<256, 1>(P, S, st, launch);
+            if (v == 6) return launch_pair<384, 1>(P, S, st, launch);
+            if (v == 7) return launch_pair<448, 1>(P, S, st, launch);
+            if (v == 8) return launch_pair<512, 1>(P, S, st, launch);
             if (v == 3) return launch_lat<T, 512, 1, true>(P, S, st, launch);
             if (v == 4) return launch_lat<T, 384, 1, true>(P, S, st, launch);
             if (v == 1) return launch_lat<T, 512, 1>(P, S, st, launch);

@@ -21,7 +21,8 @@ import torch
 from . import _lib
 from .ccsd import _mp2_t1, ctypes_void
 
-FWD_F32 = {0: "256x2", 1: "512x1", 2: "384x1", 3: "512x1 x2", 4: "384x1 x2"}
+FWD_F32 = {0: "256x2", 1: "512x1", 2: "384x1", 3: "512x1 x2", 4: "384x1 x2", 5: "rows2 256x1", 6: "rows2 384x1",
+           7: "rows2 448x1", 8: "rows2 512x1"}
 FWD_F64 = {0: "512x1", 1: "256x1"}
 LAM_F32 = {0: "256x2", 1: "512x1"}
 
@@ -38,6 +39,8 @@ def describe(w):
 def t2_kernel_fp32(w):
     """Template name of the FP32 lattice T2 kernel the word selects."""
     v = w & 15
+    if v in (5, 6, 7, 8):
+        return f"k_t2_pair<{ {5: 256, 6: 384, 7: 448, 8: 512}[v] }, 1>"
     nt, mb = {0: (256, 2), 1: (512, 1), 2: (384, 1), 3: (512, 1), 4: (384, 1)}.get(v, (256, 2))
     return f"k_t2_lat<float, 7, {nt}, {mb}, {'true' if v in (3, 4) else 'false'}>"
 

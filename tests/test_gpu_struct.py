@@ -162,11 +162,13 @@ def test_lattice_t2_kernel_matches_general_kernel(L, precision, tol):
 
 
 @pytest.mark.parametrize("L", [3, 4, 5, 6])
-@pytest.mark.parametrize("shape", [1, 2, 3, 4])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_fp32_lattice_launch_shapes_match_general_kernel(L, shape):
     """Every other FP32 launch shape of the lattice T2 update (512 and 384
-    threads, scalar and packed FP32x2 sums) against the general row kernel,
-    up to rows of 209 particles per label."""
+    threads, scalar and packed FP32x2 sums, and the two-rows-per-pass kernel
+    at 256 to 512 threads, whose blocks also meet single rows at channel
+    ends) against the general row kernel, up to rows of 209 particles per
+    label."""
     _lattice_vs_general(L, "mixed", 1e-5, shape)
 
 
