@@ -178,6 +178,48 @@ def oracle_iteration(L, A=A_BENCH):
     return dt, H.p
 
 
+def oracle_tts(L, A=4, eps=1e-8):
+    """Time to solution of the CPU port of the reference CCSD (every diagram,
+    FP64 Jacobi + mixing 0.5, the NumPy solver's energy test) from the MP2
+    start at (L, A).  Returns (seconds, iterations, E_corr)."""
+    from oracle import ccsd_oracle as O
+    O.SKIP_ZERO_BLOCKS = False
+    e_ref, fock, two = build_problem(L, A, dense=True)
+    t0 = time.perf_counter()
+    e, _, _, iters, status = O.solve(fock, two, eps=eps, maxSteps=4000, max_diis=0, criterion="numpy")
+    return time.perf_counter() - t0, iters, e
+
+
+def configs_leg(dev):
+    """The A=4 configurations (L=3, 4, 5; the bench's couplings) through the
+    public ccsd_solver on host numpy inputs, wall clock of a second (warm)
+    call: FP64 with the reference's NumPy algorithm (Jacobi + mixing 0.5,
+    energy test 1e-8) at every L; at L=5 also FP64 with pulsed DIIS 8 and the
+    mixed recipe (FP32 T2 phase with DIIS 8, then FP64 steps to the same
+    test)."""
+    import torch
+    from nulattice_b200 import ccsd_solver
+    out = {}
+    for L in (3, 4, 5):
+        e_ref, fock, two = build_problem(L, 4)
+        modes = [("fp64_jacobi", dict(max_diis=0, criterion="numpy"))]
+        if L == 5:
+            modes += [("fp64_diis8", dict(max_diis=8)),
+                      ("mixed", dict(max_diis=8, precision="mixed", mixed_eps=1e-8))]
+        res = {}
+        for name, kw in modes:
+            for _ in range(2):
+                info = {}
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                e, _, _ = ccsd_solver(fock, two, eps=1e-8, maxSteps=4000, device=dev, info=info, **kw)
+                torch.cuda.synchronize(dev)
+                t = time.perf_counter() - t0
+            res[name] = {"s": t, "iterations": info["iterations"], "e_corr": e}
+        out[f"A4_L{L}"] = res
+    return out
+
+
 def project(samples, p_target, iters):
     """Time to solution at p_target from measured (p, s/iter) samples: the
     power law s = c p^x through the two largest samples, times the FP64
@@ -214,6 +256,10 @@ def run_reference(args):
         except MemoryError:
             pass
     val, x = project(list(samples.values()), p6, FP64_ITERS_L6_MEASURED)
+    configs = {}
+    for L in (3, 4):
+        dt, iters, e = oracle_tts(L)
+        configs[f"A4_L{L}"] = {"s": dt, "iterations": iters, "e_corr": e}
     sample = (f"measured one Jacobi iteration of the numpy port of the reference CCSD (every diagram) at A={A_BENCH}: "
               + ", ".join(f"L={L} (p={pp}) {ss:.2f} s" for L, (pp, ss) in sorted(samples.items()))
               + f" (L={L_SAMPLE}: median of {args.steps}); L=6 (p={p6}) projected as s/iter ~ p^{x:.2f} "
@@ -228,6 +274,9 @@ def run_reference(args):
                       "path": "the reference's CPU algorithm (FP64 Jacobi + mixing, every diagram)"},
            "measured_s_per_iter": {f"L{L}": ss for L, (pp, ss) in sorted(samples.items())},
            "projection": {"target_L": L_BENCH, "exponent": x, "fp64_iterations": FP64_ITERS_L6_MEASURED},
+           "configs_time_to_solution": {"measured": configs,
+                                        "path": "FP64 Jacobi + mixing 0.5 from the MP2 start, energy test 1e-8, "
+                                                "A=4, C2=-3, C3=+1"},
            "cpu_baseline": {"value": val, "unit": "s", "cores": threads, "cpu": cpu_model(), "kind": "port",
                             "sample": sample},
            "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -270,6 +319,31 @@ def profile_gemm(dev, reps=10):
             outs[path] = C
         res["max_rel_err"] = float((outs["tensor_cores"] - outs["fp64"]).abs().max() / outs["fp64"].abs().max())
         out[name] = res
+    # open-shell 3He (three nucleons on one site: ring and quadratic diagrams
+    # are real contractions), ccsd_solver to 1e-10 through the general engine,
+    # mixed (tensor-core phase to the default 1e-6, then FP64) against FP64;
+    # wall clock of a second, warm call
+    from nulattice_b200 import ccsd_solver, hamiltonian as ham
+    he3 = [(0, 0, 0, 0, 0), (0, 0, 0, 1, 0), (0, 0, 0, 0, 1)]
+    for L in (4, 6):
+        e_ref, fock, two = ham.normal_ordered_hamiltonian(L, he3, -8.0, -8.0, 5.5)
+        res = {}
+        for prec in ("mixed", "fp64"):
+            for _ in range(2):
+                info = {}
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                e, _, _ = ccsd_solver(fock, two, eps=1e-10, maxSteps=3000, max_diis=8, device=dev,
+                                      precision=prec, info=info)
+                torch.cuda.synchronize()
+                t = time.perf_counter() - t0
+            res[prec] = {"s": t, "s_per_iter": t / max(1, info.get("iterations") or 1),
+                         "iterations": info.get("iterations"), "mixed_iters": info.get("mixed_iters"),
+                         "tc_gemms": info.get("tc_gemms"), "gemms": info.get("gemms"), "e_corr": e,
+                         "status": info.get("status")}
+        res["speedup"] = res["fp64"]["s"] / res["mixed"]["s"]
+        res["e_diff"] = abs(res["mixed"]["e_corr"] - res["fp64"]["e_corr"])
+        out[f"he3_L{L}_solve"] = res
     print(json.dumps({"profile_gemm": out}), flush=True)
 
 
@@ -509,14 +583,19 @@ def main():
         out["e2e"] = e2e_leg(args, fock, two, dev)
     if not args.no_adjoint:
         out["adjoint"] = adjoint_leg(dev)
+    if rank == 0:
+        out["configs"] = configs_leg(dev)
     batch = batch_leg(dev, peak, rank, ws) if not args.no_batch else None
     if not args.no_cpu and rank == 0:
         # one iteration each at L=3 and L=4 (about 10-15 s of CPU work), the
         # L=6 time to solution projected with the exponent they give
         samples = [oracle_iteration(L)[::-1] for L in (3, L_SAMPLE)]
         val, x = project(samples, plan.p, it_fp64)
+        c1 = oracle_tts(3)
         out["cpu_baseline"] = {"value": val, "unit": "s", "cores": os.cpu_count(), "cpu": cpu_model(),
                                "kind": "port", "projected": True,
+                               "measured_time_to_solution_A4_L3": {"s": c1[0], "iterations": c1[1],
+                                                                   "e_corr": c1[2]},
                                "measured_s_per_iter": {f"L{L}": ss for L, (pp, ss) in zip((3, L_SAMPLE), samples)},
                                "sample": "measured one Jacobi iteration of the numpy port of the reference CCSD "
                                          f"(every diagram) at A={A_BENCH}, L=3 (p={samples[0][0]}) "
@@ -564,8 +643,6 @@ def batch_leg(dev, peak_gbs, rank=0, ws=1):
     t_batch = gmax(t_batch)
     res = scan.results()
     ok = [r for r in res if r["status"] == "converged" and r["lambda_status"] == "converged"]
-    failed = [{"A": r["A"], "L": r["L"], "C2": round(r["C2"], 4), "C3": round(r["C3"], 4), "status": r["status"],
-               "lambda_status": r["lambda_status"], "E_corr": round(r["E_corr"], 4)} for r in res if r not in ok]
     # algorithmic bytes of the steps that ran: 3 passes over the compact T2
     # (read, write, DIIS error) per forward or Lambda step, FP32 or FP64
     alg = 0.0
@@ -597,7 +674,22 @@ def batch_leg(dev, peak_gbs, rank=0, ws=1):
             if mode == "fp64" and g is not None and r in ok:
                 diffs.append((abs(e - r["E_corr"]) / abs(r["E_corr"]), abs(2 * g[0] - r["dE_dC2"]) / abs(r["dE_dC2"]),
                               abs(2 * g[1] - r["dE_dC3"]) / abs(r["dE_dC3"])))
+        if r not in ok:
+            # the reason: the reference's own algorithms on the same instance in
+            # FP64, ten times the batch's step limit (NumPy solver: Jacobi with
+            # mixing 0.5; torch solver: pulsed DIIS 8)
+            out = {}
+            for name, kw in (("fp64_jacobi_5000", dict(max_diis=0, criterion="numpy")),
+                             ("fp64_diis8_5000", dict(max_diis=8))):
+                info = {}
+                e, _, _ = solve_structured(x.eng, eps=1e-10, maxSteps=5000, t2_format="compact", info=info,
+                                           loop="eager", precision="fp64", **kw)
+                out[name] = {"status": info["status"], "iterations": info["iterations"], "E_corr": round(e, 4)}
+            r["reference_algorithms"] = out
     scan.close()
+    failed = [{"A": r["A"], "L": r["L"], "C2": round(r["C2"], 4), "C3": round(r["C3"], 4), "status": r["status"],
+               "lambda_status": r["lambda_status"], "E_corr": round(r["E_corr"], 4),
+               "reference_algorithms": r["reference_algorithms"]} for r in res if r not in ok]
     if ws > 1:
         gathered = B.gather_results([(res, failed, diffs, alg)])
         res = [r for g in gathered for r in g[0]]

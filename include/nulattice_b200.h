@@ -480,7 +480,9 @@ typedef struct {
 
 /* MP2 start t2 = V / (e_i + e_j - e_a - e_b + delta) (coupled_cluster.py:416-439). */
 int nlb_pw_init(const nlb_pw_problem *P, double *t2, double delta, nlb_stream_t stream);
-/* M of t2 and E = 1/4 sum v_pphh t2 into S->energy (coupled_cluster.py:265-286). */
+/* M of t2 and E = 1/4 sum v_pphh t2 into S->energy (coupled_cluster.py:265-286).
+ * S->Y holds the energy's partial sums afterwards (nlb_pw_step rebuilds Y
+ * from t2 before it reads it). */
 int nlb_pw_energy(const nlb_pw_problem *P, const double *t2, nlb_pw_state *S, nlb_stream_t stream);
 /* One Jacobi step with mixing (S->M must hold M of t2): t2_out, and
  * err = t2_out - t2 when err is not NULL. */

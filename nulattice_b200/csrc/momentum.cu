@@ -145,18 +145,34 @@ __global__ void k_pw_M(nlb_pw_problem P, const double* __restrict__ t2, double* 
     }
 }
 
-// E = 1/4 sum_K sum_{sigma, c} V[sigma][spins of c] M_K[sigma][c]; one block,
-// fixed order.
-__global__ void k_pw_energy(nlb_pw_problem P, const double* __restrict__ M, double* out) {
+// E = 1/4 sum_K sum_{sigma, c} V[sigma][spins of c] M_K[sigma][c] in two
+// launches: block x of the first adds the fixed slice x of M (its threads
+// strided, then a fixed tree) into part[x]; one block then adds the parts in
+// slice order.  The result does not depend on scheduling.
+constexpr int kPwEnergyParts = 256;
+
+__global__ void k_pw_energy_part(nlb_pw_problem P, const double* __restrict__ M, double* __restrict__ part) {
     const int64_t n = P.n_m;
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t e0 = (int64_t)blockIdx.x * chunk;
+    const int64_t e1 = e0 + chunk < n ? e0 + chunk : n;
     double acc = 0.0;
-    for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
-        const int b = seg_of(P.m_off, P.n_blocks, e);
+    int b = -1;
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        if (b < 0) b = seg_of(P.m_off, P.n_blocks, e);
+        while (e >= P.m_off[b + 1]) ++b;   // the thread's entries only move forward
         const int nc = P.blk_nc[b];
         const int64_t loc = e - P.m_off[b];
         const int sg = (int)(loc / nc), c = (int)(loc % nc);
         acc += P.V[sg * 16 + (c & 15)] * M[e];
     }
+    const double s = pw_block_sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_pw_energy_sum(const double* __restrict__ part, int n, double* out) {
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) acc += part[k];
     const double s = pw_block_sum(acc);
     if (threadIdx.x == 0) *out = 0.25 * s;
 }
@@ -202,40 +218,45 @@ __global__ void k_pw_xrow(nlb_pw_problem P, const double* __restrict__ t2, doubl
 // X_pp[m][s_b][s_c] = f_pp - 1/2 sum_K sum_{s_d} Y[(K, pa(m), s_b, s_d)][s_c]   (ccDgrams.py:502-514)
 // X_hh[m][s_k][s_j] = -f_hh - 1/2 sum_{m_l} sum_{s_l} sum_sigma
 //                     V[sigma][s_k s_l] M_{m+m_l}[sigma][(m, s_j, s_l)]       (ccDgrams.py:515-527)
+// One warp per entry: the lanes take the momentum blocks (X_pp) or the
+// (m_l, s_l) pairs (X_hh) strided, a fixed shuffle tree adds them.
 __global__ void k_pw_X(nlb_pw_problem P, const double* __restrict__ Y, const double* __restrict__ M,
                        double* __restrict__ Xpp, double* __restrict__ Xhh) {
     const int L = P.L, L3 = L * L * L;
+    const int lane = threadIdx.x & 31;
+    const int64_t wpb = blockDim.x >> 5;
     const int64_t np = (int64_t)P.n_pmom * 16, nh = (int64_t)P.n_hmom * 16;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < np + nh; e += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t e = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); e < np + nh; e += (int64_t)gridDim.x * wpb) {
+        double acc = 0.0;
         if (e < np) {
             const int m = (int)(e >> 4), sb = (int)(e >> 2) & 3, sc = (int)e & 3;
             const int k = P.pmom[m];
-            double acc = 0.0;
-            for (int b = 0; b < P.n_blocks; ++b) {
+            for (int b = lane; b < P.n_blocks; b += 32) {
                 const int pa = P.ppos[(int64_t)b * L3 + k];
                 if (pa < 0) continue;
                 const int64_t row = P.row_off[b] + pa * 16 + sb * 4;
 #pragma unroll
                 for (int sd = 0; sd < 4; ++sd) acc += Y[(row + sd) * 4 + sc];
             }
-            Xpp[e] = P.fpp[e] - 0.5 * acc;
         } else {
             const int64_t u = e - np;
             const int m = (int)(u >> 4), sk = (int)(u >> 2) & 3, sj = (int)u & 3;
             const int k = P.hmom[m];
-            double acc = 0.0;
-            for (int l = 0; l < P.n_hmom; ++l) {
+            for (int w = lane; w < 4 * P.n_hmom; w += 32) {
+                const int l = w >> 2, sl = w & 3;
                 const int b = P.kblk[madd(k, P.hmom[l], L)];
                 const int pj = P.hpos[(int64_t)b * L3 + k];
                 const int nc = P.blk_nc[b];
                 const double* Mb = M + P.m_off[b];
-                for (int sl = 0; sl < 4; ++sl) {
-                    const int col = pj * 16 + sj * 4 + sl;
+                const int col = pj * 16 + sj * 4 + sl;
 #pragma unroll 4
-                    for (int sg = 0; sg < 16; ++sg) acc += P.V[sg * 16 + sk * 4 + sl] * Mb[(int64_t)sg * nc + col];
-                }
+                for (int sg = 0; sg < 16; ++sg) acc += P.V[sg * 16 + sk * 4 + sl] * Mb[(int64_t)sg * nc + col];
             }
-            Xhh[u] = -P.fhh[u] - 0.5 * acc;
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            if (e < np) Xpp[e] = P.fpp[e] - 0.5 * acc;
+            else Xhh[e - np] = -P.fhh[e - np] - 0.5 * acc;
         }
     }
 }
@@ -445,11 +466,14 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
 __global__ void k_pw_jacobi(nlb_pw_problem P, const double* __restrict__ t2, const double* __restrict__ H,
                             const double* __restrict__ Xpp, const double* __restrict__ Xhh, double mixing,
                             double* __restrict__ out, double* __restrict__ err) {
+    // grid (chunks, momentum blocks): blockIdx.y is the block of t2
     const int L = P.L, L3 = L * L * L;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < P.n_t2; e += (int64_t)gridDim.x * blockDim.x) {
-        const int b = seg_of(P.blk_off, P.n_blocks, e);
-        const int64_t loc = e - P.blk_off[b];
-        const int nc = P.blk_nc[b];
+    const int b = blockIdx.y;
+    const int64_t boff = P.blk_off[b], bn = P.blk_off[b + 1] - boff;
+    const int nc = P.blk_nc[b];
+    for (int64_t loc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; loc < bn;
+         loc += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = boff + loc;
         const Amp A = decode_amp(P, b, (int)(loc / nc), (int)(loc % nc));
         const int rb = P.ppos[(int64_t)b * L3 + P.pmom[A.mb]] * 16 + A.sb * 4 + A.sa;
         const int cj = P.hpos[(int64_t)b * L3 + P.hmom[A.mj]] * 16 + A.sj * 4 + A.si;
@@ -486,10 +510,16 @@ int nlb_pw_init(const nlb_pw_problem* P, double* t2, double delta, nlb_stream_t 
 }
 
 int nlb_pw_energy(const nlb_pw_problem* P, const double* t2, nlb_pw_state* S, nlb_stream_t stream) {
-    if (!pw_ok(P) || !t2 || !S || !S->M || !S->energy) return pfail(NLB_ERR_ARG, "nlb_pw_energy: bad argument");
+    if (!pw_ok(P) || !t2 || !S || !S->M || !S->Y || !S->energy)
+        return pfail(NLB_ERR_ARG, "nlb_pw_energy: bad argument");
     cudaStream_t st = (cudaStream_t)stream;
     k_pw_M<<<pgrid(32 * P->n_m), 256, 0, st>>>(*P, t2, S->M);
-    k_pw_energy<<<1, 256, 0, st>>>(*P, S->M, S->energy);
+    // the partial sums go to S->Y (rebuilt from t2 by every step before use)
+    int64_t nparts = 4 * P->n_rows;
+    if (nparts > kPwEnergyParts) nparts = kPwEnergyParts;
+    if (nparts > P->n_m) nparts = P->n_m;
+    k_pw_energy_part<<<(unsigned)nparts, 256, 0, st>>>(*P, S->M, S->Y);
+    k_pw_energy_sum<<<1, 256, 0, st>>>(S->Y, (int)nparts, S->energy);
     return pcheck("nlb_pw_energy");
 }
 
@@ -498,10 +528,11 @@ int nlb_pw_step(const nlb_pw_problem* P, const double* t2, double* t2_out, doubl
     if (!pw_ok(P) || !t2 || !t2_out || t2 == t2_out || !S || !S->M || !S->W || !S->Y || !S->Xpp || !S->Xhh || !S->R ||
         !S->U || !S->G || !S->H)
         return pfail(NLB_ERR_ARG, "nlb_pw_step: bad argument");
+    if (P->n_blocks > 65535) return pfail(NLB_ERR_SIZE, "nlb_pw_step: more than 65535 momentum blocks");
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t nph = (int64_t)(4 * P->n_pmom) * (4 * P->n_hmom);
     k_pw_xrow<<<pgrid(32 * P->n_rows), 256, 0, st>>>(*P, t2, S->Y);
-    k_pw_X<<<pgrid(16 * (int64_t)(P->n_pmom + P->n_hmom)), 256, 0, st>>>(*P, S->Y, S->M, S->Xpp, S->Xhh);
+    k_pw_X<<<pgrid(32 * 16 * (int64_t)(P->n_pmom + P->n_hmom)), 256, 0, st>>>(*P, S->Y, S->M, S->Xpp, S->Xhh);
     k_pw_W<<<pgrid(P->n_w), 256, 0, st>>>(*P, S->M, S->W);
     k_pw_R<<<pgrid(nph), 256, 0, st>>>(*P, t2, S->R, S->U, S->G);
     int rc = pcheck("nlb_pw_step (intermediates)");
@@ -509,7 +540,10 @@ int nlb_pw_step(const nlb_pw_problem* P, const double* t2, double* t2_out, doubl
     if (P->n_tiles > 0)
         k_pw_residual<<<P->n_tiles < 65535 ? P->n_tiles : 65535, 256, 0, st>>>(*P, t2, S->M, S->W, S->Xpp, S->Xhh,
                                                                                S->R, S->U, S->G, S->H);
-    k_pw_jacobi<<<pgrid(P->n_t2), 256, 0, st>>>(*P, t2, S->H, S->Xpp, S->Xhh, mixing, t2_out, err);
+    int64_t gx = 2 * ((P->n_t2 / P->n_blocks + 255) / 256);
+    gx = gx < 1 ? 1 : (gx > 64 ? 64 : gx);
+    k_pw_jacobi<<<dim3((unsigned)gx, (unsigned)P->n_blocks), 256, 0, st>>>(*P, t2, S->H, S->Xpp, S->Xhh, mixing,
+                                                                         t2_out, err);
     return pcheck("nlb_pw_step");
 }
 

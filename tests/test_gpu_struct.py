@@ -86,6 +86,27 @@ def test_a28_two_steps_match_reference():
     assert np.linalg.norm(t2) == pytest.approx(float(g["traj_t2_norm"]), rel=1e-11)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_a28_tight_fixed_point_matches_reference(precision):
+    """A=28 (seven closed sites), L=4: the fixed point of the reference's own
+    NumPy solver (eps 1e-13, 141 Jacobi steps, Jacobi gap 1e-12).  The
+    structured engine with pulsed DIIS, FP64 throughout or FP32 T2 to 1e-8
+    and then FP64, reaches it within 1e-10 (the FP32 phase alone within
+    1e-6)."""
+    g = G.load("a28_L4_tight")
+    fock, two = G.hamiltonian(g)
+    ref = float(g["tight_e"])
+    info = {}
+    kw = dict(precision="mixed", mixed_eps=1e-8) if precision == "mixed" else {}
+    e, t1, t2 = ccsd_solver(fock, two, eps=1e-13, maxSteps=3000, max_diis=8, device=DEV, info=info, **kw)
+    assert info["engine"] == "structured" and info["status"] == "converged", info
+    if precision == "mixed":
+        assert abs(info["mixed_energy"] - ref) <= 1e-6 * abs(ref), (info, ref)
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
+    np.testing.assert_allclose(t1, g["tight_t1"], atol=1e-9)
+    assert np.linalg.norm(t2) == pytest.approx(float(g["tight_t2_norm"]), rel=1e-9)
+
+
 @pytest.mark.parametrize("tag", ["he4_L3_c1", "he4_L4_c2", "he4_L5_c3"])
 def test_mixed_precision_energy(tag):
     g = G.load(tag)

@@ -20,7 +20,7 @@ def _canon(rows):
     return {k: v for k, v in d.items() if v != 0}
 
 
-@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he3_L3", "li6x_L3", "he4_L4_c2"])
+@pytest.mark.parametrize("tag", ["o16_L2", "he4_L3_c1", "he4_L3_t5", "he3_L3", "li6x_L3", "he4_L4_c2", "a28_L4_tight"])
 def test_builder_matches_reference(tag):
     g = G.load(tag)
     vs1 = float(g["vs1"]) if "vs1" in g else float(g["v2"])
@@ -248,3 +248,19 @@ def test_dense_work_size_matches_the_header():
     hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
                             "nulattice_b200.h")).read()
     assert int(re.search(r"#define NLB_DENSE_WORK_DOUBLES (\d+)", hdr).group(1)) == _lib.NLB_DENSE_WORK_DOUBLES
+
+
+def test_channel_model_a28_ten_unmixed_steps():
+    """Ten unmixed Jacobi steps of the reference's NumPy solver at A=28, L=4
+    (golden a28_L4_tight) through the CPU model of the channel kernels."""
+    g = G.load("a28_L4_tight")
+    e, fock, two = ham.normal_ordered_hamiltonian(4, g["holes"], -6.0, -6.0, 2.0, dense=False)
+    plan, _ = S.detect(fock, two)
+    H_f = [np.asarray(f) for f in fock]
+    t1 = O.t1_init(O.Hamiltonian(fock, [two[0], two[1]] + [b.to_dense() for b in two[2:]]))
+    B = np.zeros(plan.n_t2)
+    for _ in range(10):
+        t1, B = M.iterate(plan, H_f, t1, B, 0.0)
+    assert float(np.sum(H_f[1] * t1)) == pytest.approx(float(g["m0_e"]), rel=1e-12)
+    np.testing.assert_allclose(t1, g["m0_t1"], atol=1e-12)
+    assert 2.0 * np.linalg.norm(B) == pytest.approx(float(g["m0_t2_norm"]), rel=1e-11)
