@@ -127,7 +127,7 @@ class LambdaSolver:
                 _lib.check(L.nlb_lambda_diis(self.eng.prob, b["state"], max_diis, sp), "lambda_diis")
 
     def _graph(self, b, chunk, max_diis):
-        key = ("graph", chunk, max_diis)
+        key = ("graph", chunk, max_diis, int(self.eng.prob.tune))   # shapes of the tuning word
         if key not in b:
             dev = self.eng.dev
             side = torch.cuda.Stream(dev)
@@ -209,7 +209,11 @@ def lambda_gradient(eng, t1_dev, t2c_dev, derivs, tol=1e-9, mixing=0.5, max_step
             _lib.check(L.nlb_convert(b32["lam2"][c.parity].data_ptr(), _lib.NLB_F32, b64["lam2"][0].data_ptr(),
                                      _lib.NLB_F64, pl.n_t2, sp), "convert")
             keep = True
-    c = solver.run(b64, tol, mixing, max(max_steps - iters, 1), max_diis, keep=keep)
+    # continuing from converged FP32 multipliers, the FP64 phase has about two
+    # decades left: a DIIS pulse every four steps reaches them in one pulse
+    # instead of eight steps (the equations are linear)
+    diis64 = min(max_diis, 4) if keep else max_diis
+    c = solver.run(b64, tol, mixing, max(max_steps - iters, 1), diis64, keep=keep)
     iters += c.iter
     launches += solver.launches
     status = {1: "converged", 2: "max_iter", 3: "diverged"}.get(c.status, "running")

@@ -229,7 +229,7 @@ class StructuredEngine:
 
         Every kernel reads its buffer parity and status from the device, so
         the same graph serves every chunk of every solve on these buffers."""
-        key = ("graph", chunk, max_diis)
+        key = ("graph", chunk, max_diis, int(self.prob.tune))
         if key in b:
             return b[key]
         dev = self.dev
@@ -257,8 +257,9 @@ class StructuredEngine:
         returns (ctrl of the last phase, its buffers, out[8])."""
         import ctypes
         L = _lib.lib()
+        # the graph bakes in the launch shapes of the tuning word
         key = ("loop", phases, float(eps), float(mixed_eps), float(mixing), int(max_steps), int(criterion),
-               int(max_diis), int(chunk), float(e0))
+               int(max_diis), int(chunk), float(e0), int(self.prob.tune))
         if not hasattr(self, "_loops"):
             self._loops = {}
             self._loop_t1 = torch.zeros(self.plan.p * self.plan.h, dtype=torch.float64, device=self.dev)
