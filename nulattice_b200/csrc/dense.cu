@@ -485,18 +485,31 @@ __global__ void k_unpack_c(const double* __restrict__ P, double* __restrict__ C,
     }
 }
 
-// One cuBLAS handle per device, bound to the caller's stream at each call.
+// One cuBLAS handle per device, bound to the caller's stream at each call,
+// with a workspace of its own (allocated with the handle), so that cuBLAS
+// never allocates inside a stream capture (setting the stream resets the
+// workspace to the library's pool, so it is set again after each).
 cublasHandle_t g_blas[64] = {};
+void* g_blas_ws[64] = {};
+constexpr size_t kBlasWorkspace = 32u << 20;
 
 cublasHandle_t blas_handle(cudaStream_t st) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return nullptr;
-    if (!g_blas[dev] && cublasCreate(&g_blas[dev]) != CUBLAS_STATUS_SUCCESS) {
-        g_blas[dev] = nullptr;
-        return nullptr;
+    if (!g_blas[dev]) {
+        if (cublasCreate(&g_blas[dev]) != CUBLAS_STATUS_SUCCESS) {
+            g_blas[dev] = nullptr;
+            return nullptr;
+        }
+        if (cudaMalloc(&g_blas_ws[dev], kBlasWorkspace) != cudaSuccess) {
+            cudaGetLastError();
+            g_blas_ws[dev] = nullptr;
+        }
     }
     if (cublasSetStream(g_blas[dev], st) != CUBLAS_STATUS_SUCCESS) return nullptr;
+    if (g_blas_ws[dev] && cublasSetWorkspace(g_blas[dev], g_blas_ws[dev], kBlasWorkspace) != CUBLAS_STATUS_SUCCESS)
+        return nullptr;
     return g_blas[dev];
 }
 

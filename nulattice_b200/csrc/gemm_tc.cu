@@ -434,11 +434,13 @@ int nlb_contract_gemm_tf32x3(const nlb_contract_desc* d, const double* A, const 
         !panel_map(&maps[2], bh, g.np, g.kp) || !panel_map(&maps[3], bl, g.np, g.kp))
         return gfail(NLB_ERR_CUDA, "nlb_contract_gemm_tf32x3: cuTensorMapEncodeTiled failed");
     const int smem = kStages * kStageBytes + 1024;
-    static bool attr = false;
-    if (!attr) {
+    static bool attr[64] = {};   // once per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
         if (cudaFuncSetAttribute(k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
             return gfail(NLB_ERR_CUDA, "nlb_contract_gemm_tf32x3: shared-memory attribute");
-        attr = true;
+        if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     cudaMemsetAsync(err, 0, sizeof(int), st);
     k_split_pack<<<grid1(g.mp * g.kp), 256, 0, st>>>(A, ah, al, d->M, g.mp, d->K, g.kp, *d, 0);
