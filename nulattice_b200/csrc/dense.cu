@@ -513,6 +513,32 @@ cublasHandle_t blas_handle(cudaStream_t st) {
     return g_blas[dev];
 }
 
+// Small outputs with long sums (a few output tiles, K >= kDotMinK): one block
+// per output entry, the threads strided over K, a fixed tree.  The tiled
+// kernel would give such a contraction a handful of blocks that walk K
+// serially.
+// (and at most kDotMaxMacs multiply-adds: beyond that the tiles' reuse wins)
+constexpr int64_t kDotMaxOut = 1 << 15, kDotMinK = 64, kDotMaxMacs = int64_t(1) << 26;
+
+__global__ void __launch_bounds__(256) k_contract_dot(nlb_contract_desc d, const double* __restrict__ A,
+                                                      const double* __restrict__ B, double* __restrict__ C,
+                                                      double alpha, double beta) {
+    const int64_t o = blockIdx.x;   // (batch, m, n), n fastest
+    const int64_t n = o % d.N, mb = o / d.N;
+    const int64_t m = mb % d.M, bz = mb / d.M;
+    const int64_t oa = decode(bz, d.ext_b, d.sa_b, d.nb) + decode(m, d.ext_m, d.sa_m, d.nm);
+    const int64_t ob = decode(bz, d.ext_b, d.sb_b, d.nb) + decode(n, d.ext_n, d.sb_n, d.nn);
+    double acc = 0.0;
+    for (int64_t k = threadIdx.x; k < d.K; k += blockDim.x)
+        acc = fma(A[oa + decode(k, d.ext_k, d.sa_k, d.nk)], B[ob + decode(k, d.ext_k, d.sb_k, d.nk)], acc);
+    const double s = dblock_sum(acc);
+    if (threadIdx.x == 0) {
+        double* c = C + decode(bz, d.ext_b, d.sc_b, d.nb) + decode(m, d.ext_m, d.sc_m, d.nm) +
+                    decode(n, d.ext_n, d.sc_n, d.nn);
+        *c = (beta == 0.0) ? alpha * s : alpha * s + beta * *c;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -529,6 +555,8 @@ int nlb_contract_f64(const nlb_contract_desc* d, const double* A, const double* 
     if (d->K == 0) {
         // empty sum: C = beta C (alpha * 0)
         k_contract<<<grid, 256, 0, (cudaStream_t)stream>>>(*d, A, B, C, 0.0, beta);
+    } else if (d->M * d->N * d->B <= kDotMaxOut && d->K >= kDotMinK && d->M * d->N * d->B * d->K <= kDotMaxMacs) {
+        k_contract_dot<<<(unsigned)(d->M * d->N * d->B), 256, 0, (cudaStream_t)stream>>>(*d, A, B, C, alpha, beta);
     } else {
         k_contract<<<grid, 256, 0, (cudaStream_t)stream>>>(*d, A, B, C, alpha, beta);
     }
