@@ -557,7 +557,7 @@ def main():
            "config": {"workload": "ccsd_L6_A28_mixed", "L": L_BENCH, "A": A_BENCH, "p": plan.p, "h": plan.h,
                       "C2": C2, "C3": C3, "units": "hbar^2/(M a^2)", "n_t2_compact": n_t2,
                       "tune": {"word": int(eng.prob.tune), "choice": T.describe(int(eng.prob.tune)),
-                               "measured_us": tune_info.get("us"), "cached": tune_info.get("cached")},
+                               "cached": tune_info.get("cached")},
                       "max_diis": 8, "mixed_eps": 1e-8, "refine": refine,
                       "l2": "256 MiB flush write before every timed solve (excluded from step time)",
                       "parallelism": "replicas" if ws > 1 else "single"},
@@ -572,12 +572,11 @@ def main():
            "speedup_mixed_vs_fp64_diis": paths["fp64_diis"]["time_to_solution_s"] / tts_mixed,
            "e_ccsd": (e_corr + e_ref), "e_ccsd_fp64_fixed_point": e_tight + e_ref,
            "e_ccsd_rel_err": rel,
-           "accuracy_reference": "the FP64 structured engine at eps 1e-12 (tight FP64 fixed point, untimed); the "
-                                 "reference's own solver cannot run at L=6 (dense T2 of 4.4 GB, ~50 GB RSS, "
-                                 "~13 min per iteration), and no plain FP64 torch CCSD fits at this size either; "
-                                 "the engine is pinned to the reference's tight fixed points at A=4, L=3-5 and "
-                                 "A=28, L=4 by the GPU tests",
-           "roofline": roofline, "gpu_launches": m_launch, "clocks": clocks}
+           "accuracy_reference": "FP64 engine at eps 1e-12 (the reference cannot run at L=6: ~50 GB RSS, ~13 "
+                                 "min/iteration); the engine is pinned to the reference's tight fixed points at "
+                                 "A=4, L=3-5 and A=28, L=4 by the GPU tests",
+           "roofline": roofline, "gpu_launches": m_launch, "clocks": clocks,
+           "tune_us": tune_info.get("us")}
 
     if not args.no_e2e:
         out["e2e"] = e2e_leg(args, fock, two, dev)
@@ -603,7 +602,17 @@ def main():
                                          f"{samples[1][1]:.2f} s; L=6 (p={plan.p}) projected as s/iter ~ "
                                          f"p^{x:.2f} x {it_fp64} FP64 iterations"}
     if batch is not None:
-        out["batch"] = batch       # last: the longest block
+        out["batch"] = batch
+    # the contract keys and the short summaries first, the long detail blocks
+    # (per-path results, configurations, tuner timings, batch) last
+    first = ["metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+             "vs_baseline", "dtype", "data", "config", "roofline", "gpu_launches", "clocks", "e2e", "cpu_baseline",
+             "adjoint", "s_per_iter", "iterations", "mixed_iters", "refine_iters", "e_ccsd_rel_err",
+             "speedup_mixed_vs_fp64", "speedup_mixed_vs_fp64_diis"]
+    last = ["fp64", "fp64_diis", "mixed32", "mixed_tight", "configs", "tune_us", "batch"]
+    out = {**{k: out[k] for k in first if k in out},
+           **{k: v for k, v in out.items() if k not in first and k not in last},
+           **{k: out[k] for k in last if k in out}}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if ws > 1:
@@ -687,9 +696,12 @@ def batch_leg(dev, peak_gbs, rank=0, ws=1):
                 out[name] = {"status": info["status"], "iterations": info["iterations"], "E_corr": round(e, 4)}
             r["reference_algorithms"] = out
     scan.close()
-    failed = [{"A": r["A"], "L": r["L"], "C2": round(r["C2"], 4), "C3": round(r["C3"], 4), "status": r["status"],
-               "lambda_status": r["lambda_status"], "E_corr": round(r["E_corr"], 4),
-               "reference_algorithms": r["reference_algorithms"]} for r in res if r not in ok]
+    # one compact record per failure: the instance, the batch's statuses and
+    # E_corr, and [status, steps, E_corr] of the reference's two algorithms
+    failed = [{"inst": [r["A"], r["L"], round(r["C2"], 4), round(r["C3"], 4)],
+               "batch": [r["status"], r["lambda_status"], round(r["E_corr"], 3)],
+               **{k: [v["status"], v["iterations"], round(v["E_corr"], 3)]
+                  for k, v in r["reference_algorithms"].items()}} for r in res if r not in ok]
     if ws > 1:
         gathered = B.gather_results([(res, failed, diffs, alg)])
         res = [r for g in gathered for r in g[0]]
