@@ -149,8 +149,8 @@ __global__ void k_antisym_acc(const double* __restrict__ Z, double* __restrict__
 // orbit {abij, baij, abji, baji} (a < b, i < j); the grouping makes the
 // result exactly antisymmetric in floating point and leaves an exactly
 // antisymmetric H unchanged, so it only removes the rounding-level symmetric
-// part that atomics-ordered sums leave behind (the Jacobi map amplifies that
-// part; the reference's sequential sums never create it).
+// part that sums taken in different orders for the four images of an orbit
+// leave behind (the Jacobi map amplifies that part).
 __global__ void k_antisym_project(double* H, int64_t p, int64_t h) {
     const int64_t np = p * (p - 1) / 2, nh = h * (h - 1) / 2;
     const int64_t n = np * nh;

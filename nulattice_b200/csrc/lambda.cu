@@ -71,8 +71,14 @@ __host__ __device__ inline int64_t col_items_max(const nlb_struct_problem& P) {
     return (int64_t)P.n_channels * ((np + kColNB - 1) / kColNB) * kMaxColChunks;
 }
 
+// General path (FP64, any hole counts): the row kernel writes, per row task,
+// its Z1 contributions of particle a' into Y1r (as on the lattice path), its
+// contributions to the particles b' of label g2 into Yg (the row's own
+// [b'][k'] slice at the channel's T2 offset: n_t2 doubles cover every
+// channel), and its X_hh contractions into Tg[row][side][k'][m'] (max_nh^2
+// per side); k_l_rows_reduce adds them in a fixed order into Y1 and T.
 struct LView {
-    double *Y1, *U, *T, *fc, *Y1r, *Y1c, *Tp;
+    double *Y1, *U, *T, *fc, *Y1r, *Y1c, *Tp, *Yg, *Tg;
 };
 
 __host__ __device__ inline LView lview(double* acc, const nlb_struct_problem& P) {
@@ -84,6 +90,8 @@ __host__ __device__ inline LView lview(double* acc, const nlb_struct_problem& P)
     v.Y1r = v.fc + P.n_t1c;
     v.Y1c = v.Y1r + P.n_f2;
     v.Tp = v.Y1c + (int64_t)kMaxColChunks * P.n_f2;
+    v.Yg = v.Tp + col_items_max(P) * 2 * kLHP_;   // general path only
+    v.Tg = v.Yg + P.n_t2;
     return v;
 }
 
@@ -245,7 +253,9 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
                 const int hp = ip * nh2 + kq;
                 lt += lrow[bp * nhp + hp] * (shh[hp] + cpp) * st1a[ip];
             }
-            atomicAdd(&V.Y1[(int64_t)P.p_ord[ch.pb2 + bp] * h + P.h_ord[ch.hb2 + kq]], lt - s);
+            // (a channel without holes on the a side has no T2 block, adds
+            // nothing and owns no slots)
+            if (nh1 > 0) V.Yg[ch.offset + ((int64_t)ap * np2 + bp) * nh2 + kq] = lt - s;
         }
         // X_hh contractions T along i (g1) and along j (g2)
         for (int w = tid; w < nh1 * nh1 + nh2 * nh2; w += nt) {
@@ -255,14 +265,14 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
                 for (int bp = 0; bp < np2; ++bp)
                     for (int jq = 0; jq < nh2; ++jq)
                         s += lrow[bp * nhp + iq * nh2 + jq] * brow[bp * nhp + kq * nh2 + jq];
-                atomicAdd(&V.T[(int64_t)P.h_ord[ch.hb1 + kq] * h + P.h_ord[ch.hb1 + iq]], s);
+                V.Tg[((int64_t)task * 2 + 0) * mh * mh + kq * mh + iq] = s;
             } else {
                 const int w2 = w - nh1 * nh1;
                 const int kq = w2 / nh2, jq = w2 - kq * nh2;
                 for (int bp = 0; bp < np2; ++bp)
                     for (int iq = 0; iq < nh1; ++iq)
                         s += lrow[bp * nhp + iq * nh2 + jq] * brow[bp * nhp + iq * nh2 + kq];
-                atomicAdd(&V.T[(int64_t)P.h_ord[ch.hb2 + kq] * h + P.h_ord[ch.hb2 + jq]], s);
+                V.Tg[((int64_t)task * 2 + 1) * mh * mh + kq * mh + jq] = s;
             }
         }
         // particle a' of label g1: -sum_e Lam Ga[k'] and the ladder t1 term
@@ -281,7 +291,10 @@ __global__ void __launch_bounds__(kThreads) k_l_rows(nlb_struct_problem P, nlb_l
                 }
             }
             const double tot = block_sum(part);
-            if (tid == 0) atomicAdd(&V.Y1[(int64_t)a * h + P.h_ord[ch.hb1 + (q % nh1)]], tot);
+            if (tid == 0) {
+                double* y = V.Y1r + ch.f2_off + (int64_t)ap * nh1 + (q % nh1);
+                *y = q < nh1 ? tot : *y + tot;   // the two parts of (a', k') in a fixed order
+            }
         }
         __syncthreads();
     }
@@ -323,6 +336,53 @@ __global__ void k_l_u(nlb_struct_problem P, nlb_lambda_state S) {
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < hh + ph; u += stride) {
         if (u < hh) V.T[u] = 0.0;
         else V.Y1[u - hh] = 0.0;
+    }
+}
+
+// General path: Y1 and T from the row kernel's slots.  Thread per entry of
+// Y1 (p*h) or T (h*h); the channels in order, the rows of a channel in order.
+__global__ void k_l_rows_reduce(nlb_struct_problem P, nlb_lambda_state S) {
+    const nlb_ctrl* c = S.ctrl;
+    if (c->status != NLB_RUNNING) return;
+    const LView V = lview(S.acc, P);
+    const int h = P.h, mh = P.max_nh;
+    const int64_t ph = (int64_t)P.p * h, hh = (int64_t)h * h;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < ph + hh;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        if (idx < ph) {
+            const int x = (int)(idx / h), mm = (int)(idx % h);
+            const int g = P.p_label[x];
+            double y = 0.0;
+            if (P.h_label[mm] == g) {
+                const int xl = P.p_loc[x], ml = P.h_loc[mm];
+                for (int ci = 0; ci < P.n_channels; ++ci) {
+                    const nlb_channel& ch = P.chan[ci];
+                    if (ch.g1 == g) y += V.Y1r[ch.f2_off + (int64_t)xl * ch.nh1 + ml];
+                    if (ch.g2 == g && ch.nh1 > 0)
+                        for (int ap = 0; ap < ch.np1; ++ap)
+                            y += V.Yg[ch.offset + ((int64_t)ap * ch.np2 + xl) * ch.nh2 + ml];
+                }
+            }
+            V.Y1[idx] = y;
+        } else {
+            const int64_t u = idx - ph;
+            const int k = (int)(u / h), mm = (int)(u % h);
+            const int g = P.h_label[k];
+            double t = 0.0;
+            if (P.h_label[mm] == g) {
+                const int kl = P.h_loc[k], ml = P.h_loc[mm];
+                for (int ci = 0; ci < P.n_channels; ++ci) {
+                    const nlb_channel& ch = P.chan[ci];
+                    const int64_t t0 = ci ? P.row_end[ci - 1] : 0;
+                    for (int side = 0; side < 2; ++side) {
+                        if ((side ? ch.g2 : ch.g1) != g) continue;
+                        for (int ap = 0; ap < ch.np1; ++ap)
+                            t += V.Tg[((t0 + ap) * 2 + side) * mh * mh + kl * mh + ml];
+                    }
+                }
+            }
+            V.T[u] = t;
+        }
     }
 }
 
@@ -521,7 +581,8 @@ __global__ void k_l_setup_lat(nlb_struct_problem P, nlb_lambda_state S) {
 //   Y1[b', k']      += Lam[a'][b'][(i', k')] (v_hh + v_pp) t1[a', i'] - Lam[a'][b'][hp] Gb[a'][k'][hp]
 //   T[k', i'] (g1)  += Lam[a'][b'][i', j'] B[a'][b'][k', j']
 //   T[k', j'] (g2)  += Lam[a'][b'][i', j'] B[a'][b'][i', k']
-// and adds its partial sums with atomics (Ha is zeroed before the pass).
+// and writes its partial sums into slots with one writer each (Ha per row
+// chunk, Y1 per chunk, T per block), added in a fixed order afterwards.
 constexpr int kColRows = 256;          // most rows in one chunk of the column pass
 
 template <typename T, int NT>
@@ -1144,8 +1205,11 @@ extern "C" {
 
 int64_t nlb_lambda_acc_len(const nlb_struct_problem* prob) {
     if (!prob) return 0;
-    return (int64_t)prob->p * prob->h + 2 * (int64_t)prob->h * prob->h + prob->n_t1c +
-           (int64_t)(1 + kMaxColChunks) * prob->n_f2 + col_items_max(*prob) * 2 * kLHP;
+    const int64_t common = (int64_t)prob->p * prob->h + 2 * (int64_t)prob->h * prob->h + prob->n_t1c +
+                           (int64_t)(1 + kMaxColChunks) * prob->n_f2 + col_items_max(*prob) * 2 * kLHP;
+    if (lattice(prob)) return common;
+    // general path: the row kernel's Yg and Tg slots
+    return common + prob->n_t2 + prob->n_rows * 2 * (int64_t)prob->max_nh * prob->max_nh;
 }
 
 int64_t nlb_lambda_ha_len(const nlb_struct_problem* prob) {
@@ -1215,6 +1279,7 @@ int nlb_lambda_step(const nlb_struct_problem* prob, const nlb_lambda_state* st, 
     if (grid > kRedSlots) grid = kRedSlots;
     if (grid < 1) grid = 1;
     k_l_rows<<<(unsigned)grid, kThreads, (size_t)sm, s>>>(*prob, *st);
+    k_l_rows_reduce<<<grid_l((int64_t)prob->p * prob->h + hh), kThreads, 0, s>>>(*prob, *st);
     const int n1 = grid_l((int64_t)prob->p * prob->h);
     k_l_t1<<<n1, kThreads, 0, s>>>(*prob, *st, 0);
     k_l_finish<<<1, 32, 0, s>>>(st->ctrl, prep_view(st->prep, *prob).red, n1, (int)grid);

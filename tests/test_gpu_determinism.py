@@ -1,6 +1,6 @@
 """Every engine repeats a solve bit for bit.
 
-The kernels reduce without floating-point atomics: each reducing launch
+No kernel adds floating-point numbers with atomics: each reducing launch
 writes one partial sum per block and the consumer adds them in block order,
 and the general engine gathers its sparse v_ppph / v_pppp terms in a fixed
 row order.  Two identical solves therefore give identical energies,
@@ -79,4 +79,22 @@ def test_lambda_lattice_path_repeats():
         torch.cuda.synchronize()
         runs.append((E, g2, g3, info["lambda_iters"], info.get("lambda_path")))
     assert runs[0][4] == "lattice"
+    assert runs[0] == runs[1]
+
+
+def test_lambda_general_path_repeats():
+    """One hole per label (A=4, L=4) takes the general FP64 Lambda kernels:
+    the row kernel's Z1 and X_hh contributions sit in per-row slots added in
+    a fixed order by k_l_rows_reduce, so two gradient solves agree bit for
+    bit."""
+    from nulattice_b200 import adjoint as A
+    holes = ham.closed_shell_holes(4, 4)
+    runs = []
+    for _ in range(2):
+        info = {}
+        E, g2, g3 = A.ccsd_energy_and_gradient(4, holes, -3.0, 1.0, device=DEV, precision="fp64", eps=1e-11,
+                                               lambda_tol=1e-10, info=info)
+        torch.cuda.synchronize()
+        runs.append((E, g2, g3, info["lambda_iters"], info.get("lambda_path")))
+    assert runs[0][4] == "general"
     assert runs[0] == runs[1]
