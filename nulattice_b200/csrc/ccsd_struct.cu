@@ -843,13 +843,19 @@ __global__ void __launch_bounds__(kThreads) k_t1_update(nlb_struct_problem P, nl
 // -------------------------------------------------- convergence test ----
 // One warp: the step's energy and norms from the per-block partials of the
 // T1 (n1 blocks) and T2 (n2 blocks) launches, added in slot order.
+// Launched with three warps: warp w adds one partial-sum array (energy, T1
+// step, T2 step), each in the fixed order of warp_sum_slots.
 __global__ void k_finish(nlb_ctrl* c, const double* red, int n1, int n2) {
+    __shared__ double sums[3];
     if (blockIdx.x != 0) return;
     if (c->status != NLB_RUNNING) return;
-    const double e_sum = warp_sum_slots(red + (int64_t)kRedE * kRedSlots, n1);
-    const double d1 = warp_sum_slots(red + (int64_t)kRedDt1 * kRedSlots, n1);
-    const double d2 = c->ccs ? 0.0 : warp_sum_slots(red + (int64_t)kRedDt2 * kRedSlots, n2);
+    const int w = threadIdx.x >> 5;
+    if (w == 0) sums[0] = warp_sum_slots(red + (int64_t)kRedE * kRedSlots, n1);
+    else if (w == 1) sums[1] = warp_sum_slots(red + (int64_t)kRedDt1 * kRedSlots, n1);
+    else if (w == 2) sums[2] = c->ccs ? 0.0 : warp_sum_slots(red + (int64_t)kRedDt2 * kRedSlots, n2);
+    __syncthreads();
     if (threadIdx.x != 0) return;
+    const double e_sum = sums[0], d1 = sums[1], d2 = sums[2];
     c->e_acc = e_sum;
     c->dt1_sq = d1;
     c->dt2_sq = d2;
@@ -1360,7 +1366,7 @@ void stage_t(const nlb_struct_problem* P, const nlb_struct_state* S, int stage, 
             k_t1_update<T><<<(unsigned)t1_grid<T>(P), kThreads, 0, st>>>(*P, *S);
             break;
         default:
-            k_finish<<<1, 32, 0, st>>>(S->ctrl, prep_view(S->prep, *P).red, (int)t1_grid<T>(P),
+            k_finish<<<1, 96, 0, st>>>(S->ctrl, prep_view(S->prep, *P).red, (int)t1_grid<T>(P),
                                        (int)t2_update<T>(P, S, st, false));
     }
 }

@@ -456,13 +456,17 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S, int nchunk) {
 // in the forward k_finish (a pulse when max_diis error vectors are stored).
 // One warp: the norms from the per-block partials of the T1 (n1 blocks) and
 // row (n2 blocks) launches, added in slot order.
+// Launched with four warps, one per partial-sum array, each added in the
+// fixed order of warp_sum_slots.
 __global__ void k_l_finish(nlb_ctrl* c, const double* red, int n1, int n2) {
+    __shared__ double sums[4];
     if (blockIdx.x != 0 || c->status != NLB_RUNNING) return;
-    const double d1 = warp_sum_slots(red + (int64_t)kRedDt1 * kRedSlots, n1);
-    const double l1 = warp_sum_slots(red + (int64_t)kRedNrm1 * kRedSlots, n1);
-    const double d2 = warp_sum_slots(red + (int64_t)kRedDt2 * kRedSlots, n2);
-    const double l2 = warp_sum_slots(red + (int64_t)kRedNrm2 * kRedSlots, n2);
+    const int w = threadIdx.x >> 5;
+    const int kind[4] = {kRedDt1, kRedNrm1, kRedDt2, kRedNrm2};
+    if (w < 4) sums[w] = warp_sum_slots(red + (int64_t)kind[w] * kRedSlots, w < 2 ? n1 : n2);
+    __syncthreads();
     if (threadIdx.x != 0) return;
+    const double d1 = sums[0], l1 = sums[1], d2 = sums[2], l2 = sums[3];
     c->dt1_sq = d1;
     c->dt2_sq = d2;
     c->e_acc = l1 + l2;
@@ -1195,7 +1199,7 @@ int lat_step(const nlb_struct_problem* P, const nlb_lambda_state* S, cudaStream_
     if (cudaPeekAtLastError() != cudaSuccess) return lcheck("nlb_lambda_step");
     const int n1 = grid_l((int64_t)P->p * P->h);
     k_l_t1<<<n1, kThreads, 0, s>>>(*P, *S, nchunk);
-    k_l_finish<<<1, 32, 0, s>>>(S->ctrl, prep_view(S->prep, *P).red, n1, n2);
+    k_l_finish<<<1, 128, 0, s>>>(S->ctrl, prep_view(S->prep, *P).red, n1, n2);
     return lcheck("nlb_lambda_step");
 }
 
@@ -1282,7 +1286,7 @@ int nlb_lambda_step(const nlb_struct_problem* prob, const nlb_lambda_state* st, 
     k_l_rows_reduce<<<grid_l((int64_t)prob->p * prob->h + hh), kThreads, 0, s>>>(*prob, *st);
     const int n1 = grid_l((int64_t)prob->p * prob->h);
     k_l_t1<<<n1, kThreads, 0, s>>>(*prob, *st, 0);
-    k_l_finish<<<1, 32, 0, s>>>(st->ctrl, prep_view(st->prep, *prob).red, n1, (int)grid);
+    k_l_finish<<<1, 128, 0, s>>>(st->ctrl, prep_view(st->prep, *prob).red, n1, (int)grid);
     return lcheck("nlb_lambda_step");
 }
 
