@@ -285,6 +285,8 @@ def ccsd_energy_and_gradient(L, holes, C2, C3, device="cuda:0", precision="fp64"
         if plan is None:
             raise ValueError(f"the adjoint needs the structured engine: {why}")
         engine = StructuredEngine(plan, fock, dev)
+        from . import tune as _tune
+        engine.prob.tune = _tune.known_word(engine)
     eng = info["engine"] = engine
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()

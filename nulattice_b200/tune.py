@@ -31,6 +31,27 @@ def word(fwd32=0, lam32=0, chunks=0, fwd64=0):
     return (fwd32 & 15) | ((lam32 & 15) << 4) | ((chunks & 255) << 8) | ((fwd64 & 15) << 16)
 
 
+def known_word(eng):
+    """Launch shapes without timing: the cached word of ``eng``'s problem
+    shape on this GPU if :func:`tune` stored one, else the shapes it picks
+    on B200 at L=6, A=28 (two-row T2 kernel with 384 threads, Lambda column
+    pass in two row chunks).  Non-lattice problems: 0 (no choices)."""
+    L = _lib.lib()
+    if not L.nlb_lambda_lattice(eng.prob):
+        return 0
+    path = _cache_path()
+    if os.path.exists(path):
+        try:
+            cache = json.load(open(path))
+            entry = cache.get(_key(eng))
+            if entry is not None:
+                return int(entry["word"])
+        except (OSError, ValueError, KeyError, TypeError):
+            pass
+    chunks = 2 if max(ch.np1 for ch in eng.plan.channels) >= 8 else 0
+    return word(fwd32=6, chunks=chunks)
+
+
 def describe(w):
     return {"t2_fp32": FWD_F32.get(w & 15), "lambda_fp32": LAM_F32.get((w >> 4) & 15),
             "lambda_chunks": (w >> 8) & 255 or "auto", "t2_fp64": FWD_F64.get((w >> 16) & 15)}
