@@ -349,8 +349,9 @@ def profile_gemm(dev, reps=10):
 
 def profile_planewave(dev, cases=None):
     """Momentum-block path on closed-shell plane waves (couplings vT1 = vS1 =
-    -4, w3 = 1): two solves to 1e-10 (pulsed DIIS 8) on a warm engine, wall
-    clock, then 20 steps timed with CUDA events."""
+    -4, w3 = 1): solves to 1e-10 (pulsed DIIS 8) on a warm engine in FP64 and
+    mixed precision (FP32 phase to 1e-8, then FP64), wall clock of the second
+    of two; then 20 steps of each precision timed with CUDA events."""
     import torch
     from nulattice_b200 import momentum as MB
     from nulattice_b200 import planewave as PW
@@ -359,26 +360,33 @@ def profile_planewave(dev, cases=None):
         V = MB.contact_tensor(L, plan.n_k, -4.0, -4.0, 1.0)
         fpp, fhh, e_ref = MB.fock_blocks(L, plan.n_k, plan.hmom, plan.pmom, -4.0, -4.0, 1.0)
         eng = MB.MomentumEngine(plan, V, fpp, fhh, dev)
-        for _ in range(2):
-            info = {}
+        for prec in ("fp64", "mixed"):
+            for _ in range(2):
+                info = {}
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                e, t2 = MB.solve(plan, V, fpp, fhh, eps=1e-10, maxSteps=1000, max_diis=8, engine=eng, info=info,
+                                 precision=prec, mixed_eps=1e-8)
+                torch.cuda.synchronize(dev)
+                t = time.perf_counter() - t0
+            print(f"L={L} A={A} n_t2={plan.n_t2} {prec} E_corr={e:.12f} {info['status']} "
+                  f"iterations={info['iterations']} (fp32 {info.get('mixed_iters', 0)}) solve_s={t:.4f}",
+                  flush=True)
+        for e_ in (eng, getattr(eng, "_f32_twin", None)):
+            if e_ is None:
+                continue
+            x, y = e_.zeros(), e_.zeros()
+            e_.init(x)
+            e_.energy(x)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            for _ in range(3):
+                e_.step(x, y)
+            ev[0].record()
+            for _ in range(20):
+                e_.step(x, y)
+            ev[1].record()
             torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
-            e, t2 = MB.solve(plan, V, fpp, fhh, eps=1e-10, maxSteps=1000, max_diis=8, engine=eng, info=info)
-            torch.cuda.synchronize(dev)
-            print(f"L={L} A={A} n_t2={plan.n_t2} E_corr={e:.12f} {info['status']} iterations={info['iterations']} "
-                  f"solve_s={time.perf_counter() - t0:.4f}", flush=True)
-        x, y = eng.zeros(), eng.zeros()
-        eng.init(x)
-        eng.energy(x)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        for _ in range(3):
-            eng.step(x, y)
-        ev[0].record()
-        for _ in range(20):
-            eng.step(x, y)
-        ev[1].record()
-        torch.cuda.synchronize(dev)
-        print(f"   step_us={ev[0].elapsed_time(ev[1]) / 20 * 1e3:.1f}", flush=True)
+            print(f"   {'fp32' if e_.f32 else 'fp64'} step_us={ev[0].elapsed_time(ev[1]) / 20 * 1e3:.1f}", flush=True)
 
 
 def main():

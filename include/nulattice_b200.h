@@ -428,6 +428,9 @@ int nlb_dense_energy_f64(const double *f_ph, const double *t1, const double *v_p
  * NLB_DENSE_WORK_DOUBLES doubles. */
 int nlb_vec_diis_f64(const double *err, const double *hist, int64_t n, int32_t m, double *work,
                      double *out, nlb_stream_t stream);
+/* The same on FP32 vectors (FP64 Gram, solve and sums; out rounded once). */
+int nlb_vec_diis_f32(const float *err, const float *hist, int64_t n, int32_t m, double *work,
+                     float *out, nlb_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * Momentum-block path: closed-shell plane-wave inputs with a contact
@@ -467,14 +470,17 @@ typedef struct {
     const double *fhh;         /* [n_hmom * 16] Fock block of each hole momentum */
 } nlb_pw_problem;
 
+/* Intermediates of the momentum-block step, all of the amplitude type of the
+ * entry point they are passed to (FP64: nlb_pw_energy / nlb_pw_step; FP32:
+ * the _f32 entry points), except `energy`, which is FP64 in both. */
 typedef struct {
-    double *M;      /* [m_off[n]]   M_K[s_c s_d][col] = sum over k_c of t2 */
-    double *W;      /* [w_off[n]]   dressed hole-hole ladder */
-    double *Y;      /* [rows * 4]   row dots for X_pp */
-    double *Xpp;    /* [n_pmom * 16] */
-    double *Xhh;    /* [n_hmom * 16] */
-    double *R, *U, *G; /* [4 n_pmom * 4 n_hmom * 16] particle-hole intermediates */
-    double *H;      /* [n_t2] residual */
+    void *M;        /* [m_off[n]]   M_K[s_c s_d][col] = sum over k_c of t2 */
+    void *W;        /* [w_off[n]]   dressed hole-hole ladder */
+    void *Y;        /* [rows * 4]   row dots for X_pp */
+    void *Xpp;      /* [n_pmom * 16] */
+    void *Xhh;      /* [n_hmom * 16] */
+    void *R, *U, *G; /* [4 n_pmom * 4 n_hmom * 16] particle-hole intermediates */
+    void *H;        /* [n_t2] residual */
     double *energy; /* [1] */
 } nlb_pw_state;
 
@@ -488,6 +494,12 @@ int nlb_pw_energy(const nlb_pw_problem *P, const double *t2, nlb_pw_state *S, nl
  * err = t2_out - t2 when err is not NULL. */
 int nlb_pw_step(const nlb_pw_problem *P, const double *t2, double *t2_out, double *err, double mixing,
                 nlb_pw_state *S, nlb_stream_t stream);
+/* The same in FP32 (amplitudes and intermediates FP32, the energy's sums
+ * FP64): the first phase of a mixed-precision plane-wave solve, which then
+ * continues in FP64 from the converted amplitudes. */
+int nlb_pw_energy_f32(const nlb_pw_problem *P, const float *t2, nlb_pw_state *S, nlb_stream_t stream);
+int nlb_pw_step_f32(const nlb_pw_problem *P, const float *t2, float *t2_out, float *err, double mixing,
+                    nlb_pw_state *S, nlb_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -202,14 +202,18 @@ def lib():
     L.nlb_antisym_project_f64.argtypes = [c_void_p, c_int64, c_int64, c_void_p]
     L.nlb_antisym_project_f64.restype = c_int32
     L.nlb_vec_diis_f64.argtypes = [c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]
+    L.nlb_vec_diis_f32.argtypes = [c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]
     for name in ("nlb_contract_f64", "nlb_antisym_acc_f64", "nlb_ppph_intermediates_f64", "nlb_pppp_ladders_f64",
-                 "nlb_jacobi_f64", "nlb_dense_energy_f64", "nlb_vec_diis_f64"):
+                 "nlb_jacobi_f64", "nlb_dense_energy_f64", "nlb_vec_diis_f64", "nlb_vec_diis_f32"):
         getattr(L, name).restype = c_int32
     L.nlb_pw_init.argtypes = [ctypes.POINTER(PwProblem), c_void_p, c_double, c_void_p]
     L.nlb_pw_energy.argtypes = [ctypes.POINTER(PwProblem), c_void_p, ctypes.POINTER(PwState), c_void_p]
     L.nlb_pw_step.argtypes = [ctypes.POINTER(PwProblem), c_void_p, c_void_p, c_void_p, c_double,
                               ctypes.POINTER(PwState), c_void_p]
-    for name in ("nlb_pw_init", "nlb_pw_energy", "nlb_pw_step"):
+    L.nlb_pw_energy_f32.argtypes = [ctypes.POINTER(PwProblem), c_void_p, ctypes.POINTER(PwState), c_void_p]
+    L.nlb_pw_step_f32.argtypes = [ctypes.POINTER(PwProblem), c_void_p, c_void_p, c_void_p, c_double,
+                                  ctypes.POINTER(PwState), c_void_p]
+    for name in ("nlb_pw_init", "nlb_pw_energy", "nlb_pw_step", "nlb_pw_energy_f32", "nlb_pw_step_f32"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

@@ -366,12 +366,14 @@ __global__ void k_sum_part(const double* part, int n, double* out) {
 // Gram matrix <e_s, e_t> of m stored error vectors: per-block partials of
 // the pairs s <= t into part[blockIdx.x * 55 + k]; k_vec_gram_reduce adds them
 // in block order into gram (row stride 16).
-__global__ void k_vec_gram(const double* E, int64_t n, int m, double* part) {
+// (FP32 vectors are widened to FP64 before the products.)
+template <typename V>
+__global__ void k_vec_gram(const V* E, int64_t n, int m, double* part) {
     double acc[55];
     for (int k = 0; k < 55; ++k) acc[k] = 0.0;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         double v[10];
-        for (int s = 0; s < m; ++s) v[s] = E[(int64_t)s * n + e];
+        for (int s = 0; s < m; ++s) v[s] = (double)E[(int64_t)s * n + e];
         int k = 0;
         for (int s = 0; s < m; ++s)
             for (int t = s; t < m; ++t) acc[k++] += v[s] * v[t];
@@ -445,12 +447,14 @@ __global__ void k_vec_diis_solve(const double* gram, int m, double* coef) {
 }
 
 // t = sum_s c_s T_s over the stored amplitudes (history slots 1..m).
-__global__ void k_vec_combine(const double* coef, const double* T, int64_t n, int m, double* out) {
+// (FP64 sums; FP32 vectors are rounded once on the store.)
+template <typename V>
+__global__ void k_vec_combine(const double* coef, const V* T, int64_t n, int m, V* out) {
     if (coef[0] == 0.0) return;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         double v = 0.0;
-        for (int s = 0; s < m; ++s) v += coef[1 + s] * T[(int64_t)s * n + e];
-        out[e] = v;
+        for (int s = 0; s < m; ++s) v += coef[1 + s] * (double)T[(int64_t)s * n + e];
+        out[e] = (V)v;
     }
 }
 
@@ -537,6 +541,20 @@ __global__ void __launch_bounds__(256) k_contract_dot(nlb_contract_desc d, const
                     decode(n, d.ext_n, d.sc_n, d.nn);
         *c = (beta == 0.0) ? alpha * s : alpha * s + beta * *c;
     }
+}
+
+// Pulsed DIIS over m stored vectors: the Gram matrix (per-block partials,
+// then pairs in block order), the bordered solve, the extrapolation.
+// work: gram [0, 256), coefficients [256, 512), Gram partials after that.
+template <typename V>
+void vec_diis(const V* err, const V* hist, int64_t n, int m, double* work, V* out, cudaStream_t s) {
+    int nb = grid1(n);
+    if (nb > kDenseSlots) nb = kDenseSlots;
+    double* part = work + 512;
+    k_vec_gram<V><<<nb, 256, 0, s>>>(err, n, m, part);
+    k_vec_gram_reduce<<<m * (m + 1) / 2, 256, 0, s>>>(part, nb, m, work);
+    k_vec_diis_solve<<<1, 32, 0, s>>>(work, m, work + 256);
+    k_vec_combine<V><<<grid1(n), 256, 0, s>>>(work + 256, hist, n, m, out);
 }
 
 }  // namespace
@@ -667,16 +685,15 @@ int nlb_dense_energy_f64(const double* f_ph, const double* t1, const double* v_p
 int nlb_vec_diis_f64(const double* err, const double* hist, int64_t n, int32_t m, double* work, double* out,
                      nlb_stream_t stream) {
     if (!err || !hist || !work || !out || m < 1 || m > 10) return dfail(NLB_ERR_ARG, "nlb_vec_diis_f64: bad argument");
-    cudaStream_t s = (cudaStream_t)stream;
-    // work: gram [0, 256), coefficients [256, 512), Gram partials after that
-    int nb = grid1(n);
-    if (nb > kDenseSlots) nb = kDenseSlots;
-    double* part = work + 512;
-    k_vec_gram<<<nb, 256, 0, s>>>(err, n, m, part);
-    k_vec_gram_reduce<<<m * (m + 1) / 2, 256, 0, s>>>(part, nb, m, work);
-    k_vec_diis_solve<<<1, 32, 0, s>>>(work, m, work + 256);
-    k_vec_combine<<<grid1(n), 256, 0, s>>>(work + 256, hist, n, m, out);
+    vec_diis(err, hist, n, m, work, out, (cudaStream_t)stream);
     return dcheck("nlb_vec_diis_f64");
+}
+
+int nlb_vec_diis_f32(const float* err, const float* hist, int64_t n, int32_t m, double* work, float* out,
+                     nlb_stream_t stream) {
+    if (!err || !hist || !work || !out || m < 1 || m > 10) return dfail(NLB_ERR_ARG, "nlb_vec_diis_f32: bad argument");
+    vec_diis(err, hist, n, m, work, out, (cudaStream_t)stream);
+    return dcheck("nlb_vec_diis_f32");
 }
 
 }  // extern "C"

@@ -128,7 +128,8 @@ __global__ void k_pw_init(nlb_pw_problem P, double* t2, double delta) {
 // ------------------------------------------------------------ M, energy ----
 // M_K[sigma][c] = sum_pa T_K[pa*16 + sigma][c]: one warp per entry, the
 // lanes over the row groups pa, summed by a fixed shuffle tree.
-__global__ void k_pw_M(nlb_pw_problem P, const double* __restrict__ t2, double* __restrict__ M) {
+template <typename F>
+__global__ void k_pw_M(nlb_pw_problem P, const F* __restrict__ t2, F* __restrict__ M) {
     const int lane = threadIdx.x & 31;
     const int64_t wpb = blockDim.x >> 5;
     for (int64_t e = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); e < P.n_m; e += (int64_t)gridDim.x * wpb) {
@@ -137,8 +138,8 @@ __global__ void k_pw_M(nlb_pw_problem P, const double* __restrict__ t2, double* 
         const int64_t loc = e - P.m_off[b];
         const int sg = (int)(loc / nc), c = (int)(loc % nc);
         const int npa = P.blk_nr[b] >> 4;
-        const double* T = t2 + P.blk_off[b] + (int64_t)sg * nc + c;
-        double acc = 0.0;
+        const F* T = t2 + P.blk_off[b] + (int64_t)sg * nc + c;
+        F acc = 0.0;
         for (int pa = lane; pa < npa; pa += 32) acc += T[(int64_t)pa * 16 * nc];
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) M[e] = acc;
@@ -151,7 +152,8 @@ __global__ void k_pw_M(nlb_pw_problem P, const double* __restrict__ t2, double* 
 // slice order.  The result does not depend on scheduling.
 constexpr int kPwEnergyParts = 256;
 
-__global__ void k_pw_energy_part(nlb_pw_problem P, const double* __restrict__ M, double* __restrict__ part) {
+template <typename F>
+__global__ void k_pw_energy_part(nlb_pw_problem P, const F* __restrict__ M, double* __restrict__ part) {
     const int64_t n = P.n_m;
     const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
     const int64_t e0 = (int64_t)blockIdx.x * chunk;
@@ -164,7 +166,7 @@ __global__ void k_pw_energy_part(nlb_pw_problem P, const double* __restrict__ M,
         const int nc = P.blk_nc[b];
         const int64_t loc = e - P.m_off[b];
         const int sg = (int)(loc / nc), c = (int)(loc % nc);
-        acc += P.V[sg * 16 + (c & 15)] * M[e];
+        acc += P.V[sg * 16 + (c & 15)] * (double)M[e];
     }
     const double s = pw_block_sum(acc);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
@@ -180,8 +182,9 @@ __global__ void k_pw_energy_sum(const double* __restrict__ part, int n, double* 
 // ------------------------------------------------------------ X_pp rows ----
 // One warp per row (pa, s_b, s_d) of every block:
 //   Y[row][s_c] = sum_c V[s_c s_d][spins of c] T[row][c]
-__global__ void k_pw_xrow(nlb_pw_problem P, const double* __restrict__ t2, double* __restrict__ Y) {
-    __shared__ double Vs[256];
+template <typename F>
+__global__ void k_pw_xrow(nlb_pw_problem P, const F* __restrict__ t2, F* __restrict__ Y) {
+    __shared__ F Vs[256];
     for (int q = threadIdx.x; q < 256; q += blockDim.x) Vs[q] = P.V[q];
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -192,10 +195,10 @@ __global__ void k_pw_xrow(nlb_pw_problem P, const double* __restrict__ t2, doubl
         const int r = (int)(row - P.row_off[b]);
         const int nc = P.blk_nc[b];
         const int sd = r & 3;
-        const double* T = t2 + P.blk_off[b] + (int64_t)r * nc;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        const F* T = t2 + P.blk_off[b] + (int64_t)r * nc;
+        F a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
         for (int c = lane; c < nc; c += 32) {
-            const double x = T[c];
+            const F x = T[c];
             const int sp = c & 15;
             a0 += Vs[(0 * 4 + sd) * 16 + sp] * x;
             a1 += Vs[(1 * 4 + sd) * 16 + sp] * x;
@@ -220,14 +223,15 @@ __global__ void k_pw_xrow(nlb_pw_problem P, const double* __restrict__ t2, doubl
 //                     V[sigma][s_k s_l] M_{m+m_l}[sigma][(m, s_j, s_l)]       (ccDgrams.py:515-527)
 // One warp per entry: the lanes take the momentum blocks (X_pp) or the
 // (m_l, s_l) pairs (X_hh) strided, a fixed shuffle tree adds them.
-__global__ void k_pw_X(nlb_pw_problem P, const double* __restrict__ Y, const double* __restrict__ M,
-                       double* __restrict__ Xpp, double* __restrict__ Xhh) {
+template <typename F>
+__global__ void k_pw_X(nlb_pw_problem P, const F* __restrict__ Y, const F* __restrict__ M,
+                       F* __restrict__ Xpp, F* __restrict__ Xhh) {
     const int L = P.L, L3 = L * L * L;
     const int lane = threadIdx.x & 31;
     const int64_t wpb = blockDim.x >> 5;
     const int64_t np = (int64_t)P.n_pmom * 16, nh = (int64_t)P.n_hmom * 16;
     for (int64_t e = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); e < np + nh; e += (int64_t)gridDim.x * wpb) {
-        double acc = 0.0;
+        F acc = 0.0;
         if (e < np) {
             const int m = (int)(e >> 4), sb = (int)(e >> 2) & 3, sc = (int)e & 3;
             const int k = P.pmom[m];
@@ -247,16 +251,16 @@ __global__ void k_pw_X(nlb_pw_problem P, const double* __restrict__ Y, const dou
                 const int b = P.kblk[madd(k, P.hmom[l], L)];
                 const int pj = P.hpos[(int64_t)b * L3 + k];
                 const int nc = P.blk_nc[b];
-                const double* Mb = M + P.m_off[b];
+                const F* Mb = M + P.m_off[b];
                 const int col = pj * 16 + sj * 4 + sl;
 #pragma unroll 4
-                for (int sg = 0; sg < 16; ++sg) acc += P.V[sg * 16 + sk * 4 + sl] * Mb[(int64_t)sg * nc + col];
+                for (int sg = 0; sg < 16; ++sg) acc += F(P.V[sg * 16 + sk * 4 + sl]) * Mb[(int64_t)sg * nc + col];
             }
         }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) {
-            if (e < np) Xpp[e] = P.fpp[e] - 0.5 * acc;
-            else Xhh[e - np] = -P.fhh[e - np] - 0.5 * acc;
+            if (e < np) Xpp[e] = F(P.fpp[e]) - F(0.5) * acc;
+            else Xhh[e - np] = -F(P.fhh[e - np]) - F(0.5) * acc;
         }
     }
 }
@@ -264,18 +268,19 @@ __global__ void k_pw_X(nlb_pw_problem P, const double* __restrict__ Y, const dou
 // ---------------------------------------------------------------- W_K ----
 // W_K[c'][c] = 1/2 V[spins c'][spins c] + 1/4 sum_sigma V[sigma][spins c'] M_K[sigma][c]
 // (dgram_klij_abkl and dgram_cdkl_cdij_abkl, ccDgrams.py:240-251, 292-303)
-__global__ void k_pw_W(nlb_pw_problem P, const double* __restrict__ M, double* __restrict__ W) {
+template <typename F>
+__global__ void k_pw_W(nlb_pw_problem P, const F* __restrict__ M, F* __restrict__ W) {
     const int64_t n = P.n_w;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         const int b = seg_of(P.w_off, P.n_blocks, e);
         const int nc = P.blk_nc[b];
         const int64_t loc = e - P.w_off[b];
         const int cp = (int)(loc / nc), c = (int)(loc % nc);
-        const double* Mb = M + P.m_off[b];
-        double acc = 0.0;
+        const F* Mb = M + P.m_off[b];
+        F acc = 0.0;
 #pragma unroll 4
-        for (int sg = 0; sg < 16; ++sg) acc += P.V[sg * 16 + (cp & 15)] * Mb[(int64_t)sg * nc + c];
-        W[e] = 0.5 * P.V[(cp & 15) * 16 + (c & 15)] + 0.25 * acc;
+        for (int sg = 0; sg < 16; ++sg) acc += F(P.V[sg * 16 + (cp & 15)]) * Mb[(int64_t)sg * nc + c];
+        W[e] = F(0.5) * F(P.V[(cp & 15) * 16 + (c & 15)]) + F(0.25) * acc;
     }
 }
 
@@ -284,9 +289,10 @@ __global__ void k_pw_W(nlb_pw_problem P, const double* __restrict__ M, double* _
 //   R[s_c s_k] = sum_{k_k} t2[a, (k_k + k_i - k_a, s_c), i, (k_k, s_k)]
 //   G[s_b s_j] = - sum V[s_b s_k s_c s_j] R[s_c s_k]        (dgram_bkcj_acik, ccDgrams.py:253-264)
 //   U[s_d s_l] = sum V[s_c s_d s_k s_l] R[s_c s_k]          (dgram_cdkl_acik_dblj, ccDgrams.py:279-290)
-__global__ void k_pw_R(nlb_pw_problem P, const double* __restrict__ t2, double* __restrict__ R,
-                       double* __restrict__ U, double* __restrict__ G) {
-    __shared__ double Vs[256];
+template <typename F>
+__global__ void k_pw_R(nlb_pw_problem P, const F* __restrict__ t2, F* __restrict__ R,
+                       F* __restrict__ U, F* __restrict__ G) {
+    __shared__ F Vs[256];
     for (int q = threadIdx.x; q < 256; q += blockDim.x) Vs[q] = P.V[q];
     __syncthreads();
     const int L = P.L, L3 = L * L * L;
@@ -296,7 +302,7 @@ __global__ void k_pw_R(nlb_pw_problem P, const double* __restrict__ t2, double* 
         const int al = (int)(e / nhs), il = (int)(e % nhs);
         const int ma = al >> 2, sa = al & 3, mi = il >> 2, si = il & 3;
         const int ka = P.pmom[ma], ki = P.hmom[mi];
-        double r[16];
+        F r[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) r[q] = 0.0;
         for (int mk = 0; mk < P.n_hmom; ++mk) {
@@ -307,20 +313,20 @@ __global__ void k_pw_R(nlb_pw_problem P, const double* __restrict__ t2, double* 
             const int pa = P.ppos[(int64_t)b * L3 + ka];
             const int pi = P.hpos[(int64_t)b * L3 + ki];
             const int nc = P.blk_nc[b];
-            const double* T = t2 + P.blk_off[b] + (int64_t)(pa * 16 + sa * 4) * nc + pi * 16 + si * 4;
+            const F* T = t2 + P.blk_off[b] + (int64_t)(pa * 16 + sa * 4) * nc + pi * 16 + si * 4;
 #pragma unroll
             for (int sc = 0; sc < 4; ++sc)
 #pragma unroll
                 for (int sk = 0; sk < 4; ++sk) r[sc * 4 + sk] += T[(int64_t)sc * nc + sk];
         }
-        double* Ro = R + e * 16;
-        double* Uo = U + e * 16;
-        double* Go = G + e * 16;
+        F* Ro = R + e * 16;
+        F* Uo = U + e * 16;
+        F* Go = G + e * 16;
 #pragma unroll
         for (int q = 0; q < 16; ++q) Ro[q] = r[q];
         for (int x = 0; x < 4; ++x)
             for (int y = 0; y < 4; ++y) {
-                double g = 0.0, u = 0.0;
+                F g = 0.0, u = 0.0;
 #pragma unroll
                 for (int sc = 0; sc < 4; ++sc)
 #pragma unroll
@@ -334,14 +340,27 @@ __global__ void k_pw_R(nlb_pw_problem P, const double* __restrict__ t2, double* 
     }
 }
 
-__device__ __forceinline__ double dot16(const double* __restrict__ x, const double* __restrict__ y) {
-    double s = 0.0;
+template <typename F>
+__device__ __forceinline__ F dot16(const F* __restrict__ x, const F* __restrict__ y) {
+    F s = 0;
+    if constexpr (sizeof(F) == 8) {
 #pragma unroll
-    for (int q = 0; q < 16; q += 2) {
-        const double2 a = *reinterpret_cast<const double2*>(x + q);
-        const double2 c = *reinterpret_cast<const double2*>(y + q);
-        s += a.x * c.x;
-        s += a.y * c.y;
+        for (int q = 0; q < 16; q += 2) {
+            const double2 a = *reinterpret_cast<const double2*>(x + q);
+            const double2 c = *reinterpret_cast<const double2*>(y + q);
+            s += a.x * c.x;
+            s += a.y * c.y;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 16; q += 4) {
+            const float4 a = *reinterpret_cast<const float4*>(x + q);
+            const float4 c = *reinterpret_cast<const float4*>(y + q);
+            s += a.x * c.x;
+            s += a.y * c.y;
+            s += a.z * c.z;
+            s += a.w * c.w;
+        }
     }
     return s;
 }
@@ -356,15 +375,16 @@ __device__ __forceinline__ double dot16(const double* __restrict__ x, const doub
 // images reduce to 2 (Z(ai, bj) - Z(bi, aj)).
 constexpr int kTR = 64, kTC = 16;
 
-__global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const double* __restrict__ t2,
-                                                     const double* __restrict__ M, const double* __restrict__ W,
-                                                     const double* __restrict__ Xpp, const double* __restrict__ Xhh,
-                                                     const double* __restrict__ R, const double* __restrict__ U,
-                                                     const double* __restrict__ G, double* __restrict__ H) {
-    __shared__ double Ts[kTR][kTC + 1];
-    __shared__ double Town[kTR][kTC + 1];
-    __shared__ double Ws[kTC][kTC + 1];
-    __shared__ double Vs[256];
+template <typename F>
+__global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const F* __restrict__ t2,
+                                                     const F* __restrict__ M, const F* __restrict__ W,
+                                                     const F* __restrict__ Xpp, const F* __restrict__ Xhh,
+                                                     const F* __restrict__ R, const F* __restrict__ U,
+                                                     const F* __restrict__ G, F* __restrict__ H) {
+    __shared__ F Ts[kTR][kTC + 1];
+    __shared__ F Town[kTR][kTC + 1];
+    __shared__ F Ws[kTC][kTC + 1];
+    __shared__ F Vs[256];
     __shared__ int s_ma[4], s_mb[4], s_mi, s_mj;
     const int tid = threadIdx.x;
     const int cc = tid & 15, rr = tid >> 4;
@@ -389,9 +409,9 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
             s_mi = mi;
             s_mj = P.hinv[msub(K, P.hmom[mi], L)];
         }
-        const double* T = t2 + P.blk_off[b];
-        const double* Wb = W + P.w_off[b];
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        const F* T = t2 + P.blk_off[b];
+        const F* Wb = W + P.w_off[b];
+        F acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int k0 = 0; k0 < nc; k0 += kTC) {
             __syncthreads();
 #pragma unroll
@@ -399,7 +419,7 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
                 const int e = tid + 256 * q;
                 const int rrow = e >> 4, kk = e & 15;
                 const int r = r0 + rrow;
-                const double x = (r < nr) ? T[(int64_t)r * nc + k0 + kk] : 0.0;
+                const F x = (r < nr) ? T[(int64_t)r * nc + k0 + kk] : 0.0;
                 Ts[rrow][kk] = x;
                 if (k0 == c0) Town[rrow][kk] = x;
             }
@@ -407,21 +427,21 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
             __syncthreads();
 #pragma unroll
             for (int kk = 0; kk < kTC; ++kk) {
-                const double w = Ws[kk][cc];
+                const F w = Ws[kk][cc];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) acc[q] += Ts[rr + 16 * q][kk] * w;
             }
         }
-        const double* Mb = M + P.m_off[b];
+        const F* Mb = M + P.m_off[b];
         const int c = c0 + cc;
         const int si = (cc >> 2) & 3, sj = cc & 3, sa = (rr >> 2) & 3, sb = rr & 3;
         const int sab = sa * 4 + sb, sij = si * 4 + sj;
         const int mi = s_mi, mj = s_mj;
         // 1/2 v_pppp t2 through M: the same 16 M values for the four rows
-        double lad = 0.0;
+        F lad = 0.0;
 #pragma unroll
         for (int sg = 0; sg < 16; ++sg) lad += Vs[sab * 16 + sg] * Mb[(int64_t)sg * nc + c];
-        double xhh_j[4], xhh_i[4];
+        F xhh_j[4], xhh_i[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             xhh_j[s] = Xhh[mj * 16 + s * 4 + sj];
@@ -434,9 +454,9 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
             if (r >= nr) continue;
             const int ma = s_ma[q], mb = s_mb[q];
             // v_pphh, 1/2 v_pppp t2 (ccDgrams.py:215-237), hole-hole ladders
-            double h = Vs[sab * 16 + sij] + 0.5 * lad + acc[q];
+            F h = Vs[sab * 16 + sij] + F(0.5) * lad + acc[q];
             // P(ab) X_pp t2 and P(ij) X_hh t2 (coupled_cluster.py:536)
-            double xp = 0.0, xh = 0.0;
+            F xp = 0.0, xh = 0.0;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 xp += Xpp[mb * 16 + sb * 4 + s] * Town[q * 16 + sa * 4 + s][cc];
@@ -450,9 +470,9 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
             const int64_t i = mi * 4 + si, j = mj * 4 + sj;
             const int64_t ai = (a * nhs + i) * 16, bi = (bb * nhs + i) * 16;
             const int64_t aj = (a * nhs + j) * 16, bj = (bb * nhs + j) * 16;
-            const double ring = ((G[ai + sb * 4 + sj] - G[bi + sa * 4 + sj]) -
+            const F ring = ((G[ai + sb * 4 + sj] - G[bi + sa * 4 + sj]) -
                                  (G[aj + sb * 4 + si] - G[bj + sa * 4 + si]));
-            const double quad = dot16(U + ai, R + bj) - dot16(U + bi, R + aj);
+            const F quad = dot16(U + ai, R + bj) - dot16(U + bi, R + aj);
             h += ring + quad;
             H[P.blk_off[b] + (int64_t)r * nc + c] = h;
         }
@@ -463,9 +483,10 @@ __global__ void __launch_bounds__(256) k_pw_residual(nlb_pw_problem P, const dou
 // Exact antisymmetric projection over the orbit {abij, baij, abji, baji} (the
 // four images sit in the same block), Jacobi step with the dressed diagonal
 // denominators and mixing (coupled_cluster.py:538-545, 614-620).
-__global__ void k_pw_jacobi(nlb_pw_problem P, const double* __restrict__ t2, const double* __restrict__ H,
-                            const double* __restrict__ Xpp, const double* __restrict__ Xhh, double mixing,
-                            double* __restrict__ out, double* __restrict__ err) {
+template <typename F>
+__global__ void k_pw_jacobi(nlb_pw_problem P, const F* __restrict__ t2, const F* __restrict__ H,
+                            const F* __restrict__ Xpp, const F* __restrict__ Xhh, double mixing,
+                            F* __restrict__ out, F* __restrict__ err) {
     // grid (chunks, momentum blocks): blockIdx.y is the block of t2
     const int L = P.L, L3 = L * L * L;
     const int b = blockIdx.y;
@@ -477,15 +498,15 @@ __global__ void k_pw_jacobi(nlb_pw_problem P, const double* __restrict__ t2, con
         const Amp A = decode_amp(P, b, (int)(loc / nc), (int)(loc % nc));
         const int rb = P.ppos[(int64_t)b * L3 + P.pmom[A.mb]] * 16 + A.sb * 4 + A.sa;
         const int cj = P.hpos[(int64_t)b * L3 + P.hmom[A.mj]] * 16 + A.sj * 4 + A.si;
-        const double* Hb = H + A.off;
-        const double x_abij = Hb[loc], x_baij = Hb[(int64_t)rb * nc + A.c];
-        const double x_abji = Hb[(int64_t)A.r * nc + cj], x_baji = Hb[(int64_t)rb * nc + cj];
-        const double v = 0.25 * ((x_abij - x_baij) - (x_abji - x_baji));
-        const double den = -((Xpp[A.ma * 16 + A.sa * 5] + Xpp[A.mb * 16 + A.sb * 5]) +
+        const F* Hb = H + A.off;
+        const F x_abij = Hb[loc], x_baij = Hb[(int64_t)rb * nc + A.c];
+        const F x_abji = Hb[(int64_t)A.r * nc + cj], x_baji = Hb[(int64_t)rb * nc + cj];
+        const F v = F(0.25) * ((x_abij - x_baij) - (x_abji - x_baji));
+        const F den = -((Xpp[A.ma * 16 + A.sa * 5] + Xpp[A.mb * 16 + A.sb * 5]) +
                              (Xhh[A.mi * 16 + A.si * 5] + Xhh[A.mj * 16 + A.sj * 5]));
-        const double t = t2[e];
-        const double tn = t + v / den;
-        const double o = mixing * t + (1.0 - mixing) * tn;
+        const F t = t2[e];
+        const F tn = t + v / den;
+        const F o = F(mixing) * t + F(1.0 - mixing) * tn;
         out[e] = o;
         if (err) err[e] = o - t;
     }
@@ -499,6 +520,51 @@ bool pw_ok(const nlb_pw_problem* P) {
            P->V && P->fpp && P->fhh && (P->n_tiles == 0 || P->tiles);
 }
 
+// The energy and step entry points for amplitudes and intermediates of type
+// F (every buffer of S except `energy`, which is FP64, holds F values).
+template <typename F>
+int pw_energy(const nlb_pw_problem* P, const F* t2, nlb_pw_state* S, cudaStream_t st, const char* name) {
+    if (!pw_ok(P) || !t2 || !S || !S->M || !S->Y || !S->energy) return pfail(NLB_ERR_ARG, name);
+    F* M = static_cast<F*>(S->M);
+    k_pw_M<F><<<pgrid(32 * P->n_m), 256, 0, st>>>(*P, t2, M);
+    // the FP64 partial sums go to S->Y (rebuilt from t2 by every step
+    // before use): 4 * n_rows values of F hold 4 * n_rows * sizeof(F) / 8
+    int64_t nparts = 4 * P->n_rows * (int64_t)sizeof(F) / 8;
+    if (nparts > kPwEnergyParts) nparts = kPwEnergyParts;
+    if (nparts > P->n_m) nparts = P->n_m;
+    if (nparts < 1) nparts = 1;
+    double* part = static_cast<double*>(S->Y);
+    k_pw_energy_part<F><<<(unsigned)nparts, 256, 0, st>>>(*P, M, part);
+    k_pw_energy_sum<<<1, 256, 0, st>>>(part, (int)nparts, S->energy);
+    return pcheck(name);
+}
+
+template <typename F>
+int pw_step(const nlb_pw_problem* P, const F* t2, F* t2_out, F* err, double mixing, nlb_pw_state* S, cudaStream_t st,
+            const char* name) {
+    if (!pw_ok(P) || !t2 || !t2_out || t2 == t2_out || !S || !S->M || !S->W || !S->Y || !S->Xpp || !S->Xhh || !S->R ||
+        !S->U || !S->G || !S->H)
+        return pfail(NLB_ERR_ARG, name);
+    if (P->n_blocks > 65535) return pfail(NLB_ERR_SIZE, "momentum step: more than 65535 momentum blocks");
+    F *M = static_cast<F*>(S->M), *W = static_cast<F*>(S->W), *Y = static_cast<F*>(S->Y);
+    F *Xpp = static_cast<F*>(S->Xpp), *Xhh = static_cast<F*>(S->Xhh), *R = static_cast<F*>(S->R);
+    F *U = static_cast<F*>(S->U), *G = static_cast<F*>(S->G), *H = static_cast<F*>(S->H);
+    const int64_t nph = (int64_t)(4 * P->n_pmom) * (4 * P->n_hmom);
+    k_pw_xrow<F><<<pgrid(32 * P->n_rows), 256, 0, st>>>(*P, t2, Y);
+    k_pw_X<F><<<pgrid(32 * 16 * (int64_t)(P->n_pmom + P->n_hmom)), 256, 0, st>>>(*P, Y, M, Xpp, Xhh);
+    k_pw_W<F><<<pgrid(P->n_w), 256, 0, st>>>(*P, M, W);
+    k_pw_R<F><<<pgrid(nph), 256, 0, st>>>(*P, t2, R, U, G);
+    int rc = pcheck(name);
+    if (rc != NLB_OK) return rc;
+    if (P->n_tiles > 0)
+        k_pw_residual<F><<<P->n_tiles < 65535 ? P->n_tiles : 65535, 256, 0, st>>>(*P, t2, M, W, Xpp, Xhh, R, U, G, H);
+    int64_t gx = 2 * ((P->n_t2 / P->n_blocks + 255) / 256);
+    gx = gx < 1 ? 1 : (gx > 64 ? 64 : gx);
+    k_pw_jacobi<F><<<dim3((unsigned)gx, (unsigned)P->n_blocks), 256, 0, st>>>(*P, t2, H, Xpp, Xhh, mixing, t2_out,
+                                                                            err);
+    return pcheck(name);
+}
+
 }  // namespace
 
 extern "C" {
@@ -510,41 +576,21 @@ int nlb_pw_init(const nlb_pw_problem* P, double* t2, double delta, nlb_stream_t 
 }
 
 int nlb_pw_energy(const nlb_pw_problem* P, const double* t2, nlb_pw_state* S, nlb_stream_t stream) {
-    if (!pw_ok(P) || !t2 || !S || !S->M || !S->Y || !S->energy)
-        return pfail(NLB_ERR_ARG, "nlb_pw_energy: bad argument");
-    cudaStream_t st = (cudaStream_t)stream;
-    k_pw_M<<<pgrid(32 * P->n_m), 256, 0, st>>>(*P, t2, S->M);
-    // the partial sums go to S->Y (rebuilt from t2 by every step before use)
-    int64_t nparts = 4 * P->n_rows;
-    if (nparts > kPwEnergyParts) nparts = kPwEnergyParts;
-    if (nparts > P->n_m) nparts = P->n_m;
-    k_pw_energy_part<<<(unsigned)nparts, 256, 0, st>>>(*P, S->M, S->Y);
-    k_pw_energy_sum<<<1, 256, 0, st>>>(S->Y, (int)nparts, S->energy);
-    return pcheck("nlb_pw_energy");
+    return pw_energy<double>(P, t2, S, (cudaStream_t)stream, "nlb_pw_energy");
 }
 
 int nlb_pw_step(const nlb_pw_problem* P, const double* t2, double* t2_out, double* err, double mixing,
                 nlb_pw_state* S, nlb_stream_t stream) {
-    if (!pw_ok(P) || !t2 || !t2_out || t2 == t2_out || !S || !S->M || !S->W || !S->Y || !S->Xpp || !S->Xhh || !S->R ||
-        !S->U || !S->G || !S->H)
-        return pfail(NLB_ERR_ARG, "nlb_pw_step: bad argument");
-    if (P->n_blocks > 65535) return pfail(NLB_ERR_SIZE, "nlb_pw_step: more than 65535 momentum blocks");
-    cudaStream_t st = (cudaStream_t)stream;
-    const int64_t nph = (int64_t)(4 * P->n_pmom) * (4 * P->n_hmom);
-    k_pw_xrow<<<pgrid(32 * P->n_rows), 256, 0, st>>>(*P, t2, S->Y);
-    k_pw_X<<<pgrid(32 * 16 * (int64_t)(P->n_pmom + P->n_hmom)), 256, 0, st>>>(*P, S->Y, S->M, S->Xpp, S->Xhh);
-    k_pw_W<<<pgrid(P->n_w), 256, 0, st>>>(*P, S->M, S->W);
-    k_pw_R<<<pgrid(nph), 256, 0, st>>>(*P, t2, S->R, S->U, S->G);
-    int rc = pcheck("nlb_pw_step (intermediates)");
-    if (rc != NLB_OK) return rc;
-    if (P->n_tiles > 0)
-        k_pw_residual<<<P->n_tiles < 65535 ? P->n_tiles : 65535, 256, 0, st>>>(*P, t2, S->M, S->W, S->Xpp, S->Xhh,
-                                                                               S->R, S->U, S->G, S->H);
-    int64_t gx = 2 * ((P->n_t2 / P->n_blocks + 255) / 256);
-    gx = gx < 1 ? 1 : (gx > 64 ? 64 : gx);
-    k_pw_jacobi<<<dim3((unsigned)gx, (unsigned)P->n_blocks), 256, 0, st>>>(*P, t2, S->H, S->Xpp, S->Xhh, mixing,
-                                                                         t2_out, err);
-    return pcheck("nlb_pw_step");
+    return pw_step<double>(P, t2, t2_out, err, mixing, S, (cudaStream_t)stream, "nlb_pw_step");
+}
+
+int nlb_pw_energy_f32(const nlb_pw_problem* P, const float* t2, nlb_pw_state* S, nlb_stream_t stream) {
+    return pw_energy<float>(P, t2, S, (cudaStream_t)stream, "nlb_pw_energy_f32");
+}
+
+int nlb_pw_step_f32(const nlb_pw_problem* P, const float* t2, float* t2_out, float* err, double mixing,
+                    nlb_pw_state* S, nlb_stream_t stream) {
+    return pw_step<float>(P, t2, t2_out, err, mixing, S, (cudaStream_t)stream, "nlb_pw_step_f32");
 }
 
 }  // extern "C"

@@ -197,44 +197,58 @@ class MomentumPlan:
 
 
 class MomentumEngine:
-    """Device tables, intermediates and the three entry points
-    (``nlb_pw_init`` / ``nlb_pw_energy`` / ``nlb_pw_step``) of one problem."""
+    """Device tables, intermediates and the entry points (``nlb_pw_init`` /
+    ``nlb_pw_energy`` / ``nlb_pw_step``, or their ``_f32`` twins) of one
+    problem.  ``dtype`` is the type of the amplitudes and intermediates
+    (torch.float64, or torch.float32 for the first phase of a mixed solve);
+    ``tables``: another engine of the same problem whose device tables are
+    shared."""
 
-    def __init__(self, plan, V, fpp, fhh, device=None):
+    def __init__(self, plan, V, fpp, fhh, device=None, dtype=torch.float64, tables=None):
         self.plan = plan
         self.dev = torch.device(device if device is not None else "cuda")
         self.L = _lib.lib()
-        self.P, self._keep = plan.problem(V, fpp, fhh, self.dev)
+        if tables is not None:
+            self.P, self._keep = tables.P, tables._keep
+        else:
+            self.P, self._keep = plan.problem(V, fpp, fhh, self.dev)
+        self.dtype = dtype
+        self.f32 = dtype == torch.float32
         self.stream = torch.cuda.current_stream(self.dev)
         self.sp = ctypes.c_void_p(self.stream.cuda_stream)
         P = self.P
-        z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)  # noqa: E731
+        z = lambda k: torch.zeros(k, dtype=dtype, device=self.dev)  # noqa: E731
         nph = 4 * P.n_pmom * 4 * P.n_hmom * 16
         self.bufs = dict(M=z(P.n_m), W=z(P.n_w), Y=z(4 * P.n_rows), Xpp=z(16 * P.n_pmom), Xhh=z(16 * P.n_hmom),
-                         R=z(nph), U=z(nph), G=z(nph), H=z(plan.n_t2), energy=z(1))
+                         R=z(nph), U=z(nph), G=z(nph), H=z(plan.n_t2),
+                         energy=torch.zeros(1, dtype=torch.float64, device=self.dev))
         self.S = _lib.PwState(**{k: v.data_ptr() for k, v in self.bufs.items()})
         self.launches = 0
 
     def zeros(self):
-        return torch.zeros(self.plan.n_t2, dtype=torch.float64, device=self.dev)
+        return torch.zeros(self.plan.n_t2, dtype=self.dtype, device=self.dev)
 
     def init(self, t2, delta=0.0):
-        """MP2 start into ``t2``."""
-        _lib.check(self.L.nlb_pw_init(ctypes.byref(self.P), t2.data_ptr(), float(delta), self.sp), "pw init")
+        """MP2 start into ``t2`` (formed in FP64)."""
+        x = t2 if not self.f32 else torch.zeros(self.plan.n_t2, dtype=torch.float64, device=self.dev)
+        _lib.check(self.L.nlb_pw_init(ctypes.byref(self.P), x.data_ptr(), float(delta), self.sp), "pw init")
+        if self.f32:
+            t2.copy_(x)
         self.launches += 1
 
     def energy(self, t2):
-        """Energy of ``t2`` (device scalar); also leaves M of ``t2`` for the next step."""
-        _lib.check(self.L.nlb_pw_energy(ctypes.byref(self.P), t2.data_ptr(), ctypes.byref(self.S), self.sp),
-                   "pw energy")
-        self.launches += 2
+        """Energy of ``t2`` (device scalar, FP64); also leaves M of ``t2`` for the next step."""
+        fn = self.L.nlb_pw_energy_f32 if self.f32 else self.L.nlb_pw_energy
+        _lib.check(fn(ctypes.byref(self.P), t2.data_ptr(), ctypes.byref(self.S), self.sp), "pw energy")
+        self.launches += 3
         return self.bufs["energy"]
 
     def step(self, t2, out, err=None, mixing=0.5):
         """One Jacobi step with mixing from ``t2`` (M of ``t2`` current) into ``out``."""
-        _lib.check(self.L.nlb_pw_step(ctypes.byref(self.P), t2.data_ptr(), out.data_ptr(),
-                                      err.data_ptr() if err is not None else None, float(mixing),
-                                      ctypes.byref(self.S), self.sp), "pw step")
+        fn = self.L.nlb_pw_step_f32 if self.f32 else self.L.nlb_pw_step
+        _lib.check(fn(ctypes.byref(self.P), t2.data_ptr(), out.data_ptr(),
+                      err.data_ptr() if err is not None else None, float(mixing), ctypes.byref(self.S), self.sp),
+                   "pw step")
         self.launches += 6
 
 
@@ -247,26 +261,20 @@ def jacobi_gap(eng, t2):
     return float((out - t2).abs().max().item())
 
 
-def solve(plan, V, fpp, fhh, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5, verbose=False,
-          criterion="soa", device=None, info=None, engine=None):
-    """The solver loop of :func:`nulattice_b200.dense.solve` on the blocked
-    amplitudes.  Returns ``(E_corr, t2)``, t2 blocked on the device."""
-    info = {} if info is None else info
-    t0 = time.perf_counter()
-    eng = engine if engine is not None else MomentumEngine(plan, V, fpp, fhh, device)
+def _iterate(eng, xs, cur, eps, maxSteps, max_diis, mixing, criterion, verbose, step0=0):
+    """The solver loop on engine ``eng`` from the amplitudes ``xs[cur]``.
+    Returns (E, cur, status, steps)."""
     L, sp = eng.L, eng.sp
-    n = plan.n_t2
-    xs = [eng.zeros(), eng.zeros()]
-    cur = 0
-    eng.init(xs[0], delta)
+    n = eng.plan.n_t2
     use_diis = criterion == "soa" and max_diis > 0
     if use_diis:
-        err = torch.zeros((max_diis, n), dtype=torch.float64, device=eng.dev)
-        hist = torch.zeros((max_diis, n), dtype=torch.float64, device=eng.dev)
+        err = torch.zeros((max_diis, n), dtype=eng.dtype, device=eng.dev)
+        hist = torch.zeros((max_diis, n), dtype=eng.dtype, device=eng.dev)
         work = torch.zeros(_lib.NLB_DENSE_WORK_DOUBLES, dtype=torch.float64, device=eng.dev)
+        diis = L.nlb_vec_diis_f32 if eng.f32 else L.nlb_vec_diis_f64
         nerr = 0
     prev = float(eng.energy(xs[cur]).item())
-    if verbose:
+    if verbose and step0 == 0:
         print(f"Step 0: {prev}")
     status, e, it = "max_iter", prev, 0
     for it in range(1, maxSteps + 1):
@@ -274,7 +282,7 @@ def solve(plan, V, fpp, fhh, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mi
         cur ^= 1
         e = float(eng.energy(xs[cur]).item())
         if verbose:
-            print(f"Step {it}: {e}", "difference =", abs(e - prev) / abs(e) if e != 0 else float("inf"))
+            print(f"Step {step0 + it}: {e}", "difference =", abs(e - prev) / abs(e) if e != 0 else float("inf"))
         if criterion == "soa":
             done = abs(e - prev) / max(1.0, abs(e)) < eps
         else:
@@ -286,25 +294,63 @@ def solve(plan, V, fpp, fhh, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mi
             hist[nerr].copy_(xs[cur])
             nerr += 1
             if nerr == max_diis:
-                _lib.check(L.nlb_vec_diis_f64(err.data_ptr(), hist.data_ptr(), n, max_diis, work.data_ptr(),
-                                              xs[cur].data_ptr(), sp), "pw diis")
-                eng.launches += 3
+                _lib.check(diis(err.data_ptr(), hist.data_ptr(), n, max_diis, work.data_ptr(), xs[cur].data_ptr(),
+                                sp), "pw diis")
+                eng.launches += 4
                 eng.energy(xs[cur])    # M of the extrapolated amplitudes for the next step
                 nerr = 0
         if abs(e) > 1e10 or e != e:
             status = "diverged"
             break
         prev = e
+    return e, cur, status, it
+
+
+def solve(plan, V, fpp, fhh, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5, verbose=False,
+          criterion="soa", device=None, info=None, engine=None, precision="fp64", mixed_eps=None):
+    """The solver loop of :func:`nulattice_b200.dense.solve` on the blocked
+    amplitudes.  Returns ``(E_corr, t2)``, t2 blocked on the device (FP64).
+
+    ``precision="mixed"``: FP32 amplitudes and intermediates (FP64 energy,
+    DIIS algebra in FP64) until the energy test passes at ``mixed_eps``
+    (default ``max(eps, 1e-7)``), then FP64 from the converted amplitudes to
+    ``eps``.  ``engine``: an FP64 engine of the problem (reused)."""
+    info = {} if info is None else info
+    t0 = time.perf_counter()
+    eng = engine if engine is not None else MomentumEngine(plan, V, fpp, fhh, device)
+    xs = [eng.zeros(), eng.zeros()]
+    cur, done_steps = 0, 0
+    launches0 = eng.launches
+    if precision == "mixed":
+        e32 = getattr(eng, "_f32_twin", None)
+        if e32 is None:
+            e32 = eng._f32_twin = MomentumEngine(plan, V, fpp, fhh, eng.dev, dtype=torch.float32, tables=eng)
+        l32 = e32.launches
+        ys = [e32.zeros(), e32.zeros()]
+        e32.init(ys[0], delta)
+        me = float(mixed_eps) if mixed_eps is not None else max(float(eps), 1e-7)
+        e, c32, status, done_steps = _iterate(e32, ys, 0, me, maxSteps, max_diis, mixing, criterion, verbose)
+        info.update(mixed_iters=done_steps, mixed_energy=e, mixed_status=status)
+        launches0 -= e32.launches - l32
+        xs[0].copy_(ys[c32])
+        if status == "converged" and maxSteps - done_steps > 0:
+            e, cur, status, it = _iterate(eng, xs, 0, eps, maxSteps - done_steps, max_diis, mixing, criterion,
+                                          verbose, step0=done_steps)
+            done_steps += it
+    else:
+        eng.init(xs[0], delta)
+        e, cur, status, done_steps = _iterate(eng, xs, 0, eps, maxSteps, max_diis, mixing, criterion, verbose)
     eng.stream.synchronize()
     if status == "max_iter":
         print("Max iterations reached.")
-    info.update(status=status, iterations=it, t_iterate=time.perf_counter() - t0, launches=eng.launches,
-                engine="momentum", n_t2=n, blocks=len(plan.Ks))
+    info.update(status=status, iterations=done_steps, t_iterate=time.perf_counter() - t0,
+                launches=eng.launches - launches0, engine="momentum", n_t2=plan.n_t2, blocks=len(plan.Ks),
+                precision=precision)
     return e, xs[cur]
 
 
 def ccsd_plane_wave(L, holes, vT1, vS1, w3=0.0, eps=1e-8, maxSteps=1000, max_diis=10, delta=0.0, mixing=0.5,
-                    verbose=False, criterion="soa", device=None, info=None):
+                    verbose=False, criterion="soa", device=None, info=None, precision="fp64", mixed_eps=None):
     """CCSD of the closed-shell plane-wave Hamiltonian
     :func:`planewave.plane_wave_hamiltonian` ``(L, holes, vT1, vS1, w3)`` on
     the momentum blocks.  Returns ``(E_corr, E_ref, t2, plan)``: t2 blocked
@@ -316,5 +362,6 @@ def ccsd_plane_wave(L, holes, vT1, vS1, w3=0.0, eps=1e-8, maxSteps=1000, max_dii
     fpp, fhh, e_ref = fock_blocks(L, plan.n_k, plan.hmom, plan.pmom, vT1, vS1, w3)
     info["t_plan"] = time.perf_counter() - t0
     e, t2 = solve(plan, V, fpp, fhh, eps=eps, maxSteps=maxSteps, max_diis=max_diis, delta=delta, mixing=mixing,
-                  verbose=verbose, criterion=criterion, device=device, info=info)
+                  verbose=verbose, criterion=criterion, device=device, info=info, precision=precision,
+                  mixed_eps=mixed_eps)
     return e, e_ref, t2, plan

@@ -82,3 +82,42 @@ def test_large_closed_shell_reaches_the_fixed_point():
     pos = order[np.searchsorted(key[order], swap)]
     t = t2.cpu().numpy()
     np.testing.assert_array_equal(t[pos], -t)
+
+
+@pytest.mark.parametrize("L,A,w", [(3, 4, 0.7), (3, 28, 0.5), (6, 28, 1.0)])
+def test_mixed_precision_reaches_the_fp64_fixed_point(L, A, w):
+    """FP32 amplitudes and intermediates to |dE|/|E| < 1e-8, then FP64 from
+    the converted amplitudes: the FP64 solve's energy within 1e-10 and its
+    amplitudes within 1e-8 of their largest; the FP32 phase alone within
+    1e-6."""
+    plan, eng, (V, fpp, fhh) = _engine(L, A, -4.0, -4.0, w)
+    i64, imx = {}, {}
+    e64, t64 = MB.solve(plan, V, fpp, fhh, eps=1e-12, maxSteps=2000, max_diis=8, engine=eng, info=i64)
+    t64 = t64.clone()
+    emx, tmx = MB.solve(plan, V, fpp, fhh, eps=1e-12, maxSteps=2000, max_diis=8, engine=eng, info=imx,
+                        precision="mixed", mixed_eps=1e-8)
+    assert i64["status"] == imx["status"] == "converged", (i64, imx)
+    assert imx["mixed_iters"] > 0 and imx["mixed_status"] == "converged"
+    assert abs(imx["mixed_energy"] - e64) <= 1e-6 * abs(e64)
+    assert emx == pytest.approx(e64, rel=1e-10)
+    assert tmx.dtype == torch.float64
+    np.testing.assert_allclose(tmx.cpu().numpy(), t64.cpu().numpy(), rtol=0,
+                               atol=1e-8 * float(t64.abs().max()))
+
+
+def test_fp32_step_tracks_the_fp64_step():
+    """One FP32 step from the same amplitudes as an FP64 step: the same
+    update to FP32 rounding (the kernels are one template)."""
+    plan, eng, (V, fpp, fhh) = _engine(4, 28, -4.0, -4.0, 0.5)
+    e32 = MB.MomentumEngine(plan, V, fpp, fhh, DEV, dtype=torch.float32, tables=eng)
+    x64, y64 = eng.zeros(), eng.zeros()
+    eng.init(x64)
+    x32, y32 = e32.zeros(), e32.zeros()
+    x32.copy_(x64)
+    E64, E32 = float(eng.energy(x64).item()), float(e32.energy(x32).item())
+    eng.step(x64, y64)
+    e32.step(x32, y32)
+    torch.cuda.synchronize()
+    assert E32 == pytest.approx(E64, rel=1e-6)
+    scale = float(y64.abs().max())
+    assert float((y32.double() - y64).abs().max()) <= 1e-5 * scale
