@@ -94,6 +94,7 @@ class GpuEinsum:
         self.L = _lib.lib()
         self.sp = ctypes.c_void_p(stream_ptr)
         self._plans = {}
+        self._descs = {}
         self._ws = None
         self.launches = 0
         self.gemms = 0
@@ -107,6 +108,35 @@ class GpuEinsum:
 
     # -- one pairwise contraction ------------------------------------------
     def pair(self, spec, A, B, out, alpha=1.0, beta=0.0):
+        # the descriptor and route depend only on the spec, shapes and strides
+        key = (spec, tuple(A.shape), A.stride(), tuple(B.shape), B.stride(), tuple(out.shape), out.stride(),
+               self.tensor_cores)
+        hit = self._descs.get(key)
+        if hit is None:
+            hit = self._describe(spec, A, B, out)
+            self._descs[key] = hit
+        d, route, need = hit
+        if route == "tc":
+            ws = self._workspace(need, out.device)
+            _lib.check(self.L.nlb_contract_gemm_tf32x3(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
+                                                       alpha, beta, ws.data_ptr(), ws.numel() * 8, self.sp),
+                       "contract (tensor cores)")
+            self.launches += 4
+            self.tc_gemms += 1
+        elif route == "gemm":
+            ws = self._workspace(need, out.device)
+            _lib.check(self.L.nlb_contract_gemm_f64(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
+                                                    alpha, beta, ws.data_ptr(), ws.numel() * 8, self.sp),
+                       "contract (gemm)")
+            self.launches += 4
+            self.gemms += 1
+        else:
+            _lib.check(self.L.nlb_contract_f64(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
+                                               alpha, beta, self.sp), "contract")
+            self.launches += 1
+
+    def _describe(self, spec, A, B, out):
+        """(descriptor, route, workspace bytes) of one pairwise contraction."""
         ins, oz = spec.split("->")
         ia, ib = ins.split(",")
         d = _lib.ContractDesc()
@@ -150,25 +180,10 @@ class GpuEinsum:
         d.M, d.N, d.K, d.B = prod("m"), prod("n"), prod("k"), prod("b")
         if d.B == 1 and d.K > 0 and d.M * d.N * d.K >= GEMM_MIN_MACS:
             if self.tensor_cores and min(d.M, d.N) >= TC_MIN_MN:
-                ws = self._workspace(int(self.L.nlb_contract_gemm_tc_work(ctypes.byref(d))), out.device)
-                _lib.check(self.L.nlb_contract_gemm_tf32x3(ctypes.byref(d), A.data_ptr(), B.data_ptr(),
-                                                           out.data_ptr(), alpha, beta, ws.data_ptr(),
-                                                           ws.numel() * 8, self.sp), "contract (tensor cores)")
-                self.launches += 4
-                self.tc_gemms += 1
-                return
+                return d, "tc", int(self.L.nlb_contract_gemm_tc_work(ctypes.byref(d)))
             # large contractions: gathered panels and one library GEMM
-            need = int(self.L.nlb_contract_gemm_work(ctypes.byref(d)))
-            self._workspace(need, out.device)
-            _lib.check(self.L.nlb_contract_gemm_f64(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
-                                                    alpha, beta, self._ws.data_ptr(), self._ws.numel() * 8,
-                                                    self.sp), "contract (gemm)")
-            self.launches += 4
-            self.gemms += 1
-            return
-        _lib.check(self.L.nlb_contract_f64(ctypes.byref(d), A.data_ptr(), B.data_ptr(), out.data_ptr(),
-                                           alpha, beta, self.sp), "contract")
-        self.launches += 1
+            return d, "gemm", int(self.L.nlb_contract_gemm_work(ctypes.byref(d)))
+        return d, "tiles", 0
 
     # -- a chain of pairwise contractions ------------------------------------
     def __call__(self, spec, *ops, out, alpha=1.0, beta=0.0):
