@@ -166,21 +166,44 @@ __device__ __forceinline__ int64_t decode(int64_t lin, const int64_t* ext, const
 // tensor cores read, split into TF32 parts: hi = tf32(x), lo = tf32(x - hi)
 // with x the FP32 value.  which = 0: A[m][k] (rows m); 1: B as [n][k].
 // Rows beyond the operand and columns beyond K are zero.
-__global__ void k_split_pack(const double* __restrict__ src, float* __restrict__ hi, float* __restrict__ lo,
-                             int64_t rows, int64_t rows_pad, int64_t cols, int64_t cols_pad, nlb_contract_desc d,
-                             int which) {
-    const int64_t n = rows_pad * cols_pad;
-    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = l / cols_pad, c = l - r * cols_pad;
-        float x = 0.f;
-        if (r < rows && c < cols) {
-            const int64_t off = which == 0 ? decode(r, d.ext_m, d.sa_m, d.nm) + decode(c, d.ext_k, d.sa_k, d.nk)
-                                           : decode(c, d.ext_k, d.sb_k, d.nk) + decode(r, d.ext_n, d.sb_n, d.nn);
-            x = (float)src[off];
+// 32 x 32 tiles through shared memory: the row and column offsets are
+// decoded once per tile, and the strided side is read (or written) along
+// its contiguous index.  `*_fast`: the row index (pack: m or n; write-back:
+// m) is the contiguous one of the strided side.
+constexpr int kPT = 32;
+
+__global__ void __launch_bounds__(256) k_split_pack_t(const double* __restrict__ src, float* __restrict__ hi,
+                                                      float* __restrict__ lo, int64_t rows, int64_t rows_pad,
+                                                      int64_t cols, int64_t cols_pad, nlb_contract_desc d,
+                                                      int which, int rows_fast) {
+    __shared__ int64_t roff[kPT], coff[kPT];
+    __shared__ float tile[kPT][kPT + 1];
+    const int64_t r0 = (int64_t)blockIdx.y * kPT, c0 = (int64_t)blockIdx.x * kPT;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (threadIdx.x < kPT) {
+        const int64_t r = r0 + threadIdx.x;
+        roff[threadIdx.x] = r < rows ? (which == 0 ? decode(r, d.ext_m, d.sa_m, d.nm) : decode(r, d.ext_n, d.sb_n, d.nn))
+                                     : 0;
+    } else if (threadIdx.x < 2 * kPT) {
+        const int q = threadIdx.x - kPT;
+        const int64_t c = c0 + q;
+        coff[q] = c < cols ? (which == 0 ? decode(c, d.ext_k, d.sa_k, d.nk) : decode(c, d.ext_k, d.sb_k, d.nk)) : 0;
+    }
+    __syncthreads();
+    for (int i = ty; i < kPT; i += 8) {
+        const int rr = rows_fast ? tx : i, cc = rows_fast ? i : tx;
+        const int64_t r = r0 + rr, c = c0 + cc;
+        tile[rr][cc] = (r < rows && c < cols) ? (float)src[roff[rr] + coff[cc]] : 0.f;
+    }
+    __syncthreads();
+    for (int i = ty; i < kPT; i += 8) {
+        const int64_t r = r0 + i, c = c0 + tx;
+        if (r < rows_pad && c < cols_pad) {
+            const float x = tile[i][tx];
+            const float h = to_tf32(x);
+            hi[r * cols_pad + c] = h;
+            lo[r * cols_pad + c] = to_tf32(x - h);
         }
-        const float h = to_tf32(x);
-        hi[l] = h;
-        lo[l] = to_tf32(x - h);
     }
 }
 
@@ -188,18 +211,38 @@ __global__ void k_split_pack(const double* __restrict__ src, float* __restrict__
 // strided output; P holds `splits` partial slices [M_pad][N_pad] (split-K),
 // added in slice order in FP64.  When a tile reported a failed wait (*err)
 // every output entry becomes NaN, so the failure cannot pass unnoticed.
-__global__ void k_unpack_tile(const float* __restrict__ P, int64_t m_pad, int64_t n_pad, int splits,
-                              double* __restrict__ C, nlb_contract_desc d, double alpha, double beta,
-                              const int* err) {
-    const int64_t n = d.M * d.N;
+__global__ void __launch_bounds__(256) k_unpack_tile_t(const float* __restrict__ P, int64_t m_pad, int64_t n_pad,
+                                                       int splits, double* __restrict__ C, nlb_contract_desc d,
+                                                       double alpha, double beta, const int* err, int m_fast) {
+    __shared__ int64_t moff[kPT], noff[kPT];
+    __shared__ double tile[kPT][kPT + 1];
+    const int64_t m0 = (int64_t)blockIdx.y * kPT, n0 = (int64_t)blockIdx.x * kPT;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const bool bad = *err != 0;
-    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t m = l / d.N, q = l - m * d.N;
-        const int64_t off = decode(m, d.ext_m, d.sc_m, d.nm) + decode(q, d.ext_n, d.sc_n, d.nn);
+    if (threadIdx.x < kPT) {
+        const int64_t m = m0 + threadIdx.x;
+        moff[threadIdx.x] = m < d.M ? decode(m, d.ext_m, d.sc_m, d.nm) : 0;
+    } else if (threadIdx.x < 2 * kPT) {
+        const int q = threadIdx.x - kPT;
+        const int64_t n = n0 + q;
+        noff[q] = n < d.N ? decode(n, d.ext_n, d.sc_n, d.nn) : 0;
+    }
+    for (int i = ty; i < kPT; i += 8) {
+        const int64_t m = m0 + i, n = n0 + tx;
         double acc = 0.0;
-        for (int s = 0; s < splits; ++s) acc += (double)P[(int64_t)s * m_pad * n_pad + m * n_pad + q];
-        const double v = alpha * acc;
-        C[off] = bad ? __longlong_as_double(0x7ff8000000000000LL) : ((beta == 0.0) ? v : v + beta * C[off]);
+        if (m < d.M && n < d.N)
+            for (int s = 0; s < splits; ++s) acc += (double)P[(int64_t)s * m_pad * n_pad + m * n_pad + n];
+        tile[i][tx] = alpha * acc;
+    }
+    __syncthreads();
+    for (int i = ty; i < kPT; i += 8) {
+        const int mm = m_fast ? tx : i, nn = m_fast ? i : tx;
+        const int64_t m = m0 + mm, n = n0 + nn;
+        if (m < d.M && n < d.N) {
+            const int64_t off = moff[mm] + noff[nn];
+            const double v = tile[mm][nn];
+            C[off] = bad ? __longlong_as_double(0x7ff8000000000000LL) : ((beta == 0.0) ? v : v + beta * C[off]);
+        }
     }
 }
 
@@ -356,11 +399,6 @@ bool panel_map(CUtensorMap* m, float* base, int64_t rows, int64_t k_pad) {
 
 int64_t round_up(int64_t x, int64_t q) { return (x + q - 1) / q * q; }
 
-int grid1(int64_t n) {
-    const int64_t g = (n + 255) / 256;
-    return (int)(g < 4096 ? (g > 0 ? g : 1) : 4096);
-}
-
 int sm_count() {
     static int n = 0;
     if (n == 0) {
@@ -443,12 +481,22 @@ int nlb_contract_gemm_tf32x3(const nlb_contract_desc* d, const double* A, const 
         if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     cudaMemsetAsync(err, 0, sizeof(int), st);
-    k_split_pack<<<grid1(g.mp * g.kp), 256, 0, st>>>(A, ah, al, d->M, g.mp, d->K, g.kp, *d, 0);
-    k_split_pack<<<grid1(g.np * g.kp), 256, 0, st>>>(B, bh, bl, d->N, g.np, d->K, g.kp, *d, 1);
+    // the contiguous (innermost) index of each group: last in the decode order
+    auto unit = [](const int64_t* str, int nd) { return nd > 0 && str[nd - 1] == 1; };
+    const int a_rows_fast = unit(d->sa_m, d->nm) && !unit(d->sa_k, d->nk);
+    const int b_rows_fast = unit(d->sb_n, d->nn) && !unit(d->sb_k, d->nk);
+    const int c_m_fast = unit(d->sc_m, d->nm) && !unit(d->sc_n, d->nn);
+    if (g.mp / kPT > 65535 || g.np / kPT > 65535 || (d->M + kPT - 1) / kPT > 65535)
+        return gfail(NLB_ERR_SIZE, "nlb_contract_gemm_tf32x3: too many row tiles");
+    k_split_pack_t<<<dim3((unsigned)(g.kp / kPT), (unsigned)(g.mp / kPT)), 256, 0, st>>>(A, ah, al, d->M, g.mp, d->K,
+                                                                                      g.kp, *d, 0, a_rows_fast);
+    k_split_pack_t<<<dim3((unsigned)(g.kp / kPT), (unsigned)(g.np / kPT)), 256, 0, st>>>(B, bh, bl, d->N, g.np, d->K,
+                                                                                      g.kp, *d, 1, b_rows_fast);
     const dim3 grid((unsigned)(g.mp / kBM), (unsigned)(g.np / kBN), (unsigned)g.splits);
     k_gemm_tf32x3<<<grid, kThreads, smem, st>>>(maps[0], maps[1], maps[2], maps[3], (int)(g.kp / kBK),
                                                  g.kb_per_split, P, g.mp, g.np, err);
-    k_unpack_tile<<<grid1(d->M * d->N), 256, 0, st>>>(P, g.mp, g.np, g.splits, C, *d, alpha, beta, err);
+    k_unpack_tile_t<<<dim3((unsigned)((d->N + kPT - 1) / kPT), (unsigned)((d->M + kPT - 1) / kPT)), 256, 0, st>>>(
+        P, g.mp, g.np, g.splits, C, *d, alpha, beta, err, c_m_fast);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         char buf[256];
