@@ -171,6 +171,7 @@ __device__ __forceinline__ int64_t decode(int64_t lin, const int64_t* ext, const
 // its contiguous index.  `*_fast`: the row index (pack: m or n; write-back:
 // m) is the contiguous one of the strided side.
 constexpr int kPT = 32;
+constexpr int kGroupM = 8;   // tile rows per group of the GEMM's tile order
 
 __global__ void __launch_bounds__(256) k_split_pack_t(const double* __restrict__ src, float* __restrict__ hi,
                                                       float* __restrict__ lo, int64_t rows, int64_t rows_pad,
@@ -264,7 +265,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     __shared__ int n_issued, n_consumed;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    // tile order: groups of kGroupM tile rows, the tile columns of a group
+    // in turn, so that a wave of CTAs shares a few A panels and B panels
+    // that stay in L2 (the plain raster order streams every B panel per row)
+    int tm, tn;
+    {
+        const int tiles_m = gridDim.x, tiles_n = gridDim.y;
+        const int lin = blockIdx.y * tiles_m + blockIdx.x;
+        const int per_group = kGroupM * tiles_n;
+        const int first_m = (lin / per_group) * kGroupM;
+        const int gsize = min(tiles_m - first_m, kGroupM);
+        const int in_group = lin % per_group;
+        tm = first_m + in_group % gsize;
+        tn = in_group / gsize;
+    }
+    const int m0 = tm * kBM, n0 = tn * kBN;
     const int kb0 = blockIdx.z * kb_per_split;
     const int n_kblocks = min(kb_per_split, kb_total - kb0);
     P += (int64_t)blockIdx.z * m_pad * n_pad;
