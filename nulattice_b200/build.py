@@ -25,7 +25,8 @@ def sources():
 
 def build(force=False, verbose=False):
     srcs = sources()
-    newest = max(os.path.getmtime(s) for s in srcs + [os.path.join(ROOT, "include", "nulattice_b200.h")])
+    deps = srcs + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [os.path.join(ROOT, "include", "nulattice_b200.h")]
+    newest = max(os.path.getmtime(s) for s in deps)
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest:
         return OUT
     cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",

@@ -17,11 +17,25 @@
 // * Gb[k'][i'j'] of both rows stays in registers for the whole row pair.
 //
 // Only the f_pp neighbours along a (six L2 loads per row) stay per row.
-// A block's rows are contiguous; a row whose partner would lie in another
-// channel (or past the block's range) runs alone, its partner slot a copy
-// of it whose results are dropped.
+//
+// Work split: the passes of a channel are its rows (0, 1), (2, 3), ... and,
+// when the channel has an odd number of rows, the last row alone (its
+// partner slot a copy of it whose results are dropped).  A pass is
+// max(np2, 1) work units, one per b' column; the units of all passes, in
+// channel order, are cut into gridDim.x contiguous ranges of equal length.
+// So a block may start or end inside a pass: it then stages both rows and
+// forms Gb as a whole pass does, but updates only the b' columns of its
+// range, and the block holding column 0 writes the pass's F2 entries.  With
+// whole passes per block the rows would not divide evenly (1254 rows on 148
+// blocks at L=6: four passes on some blocks, five on others).
 
 constexpr int kPairRec = 32;   // floats per b' record
+
+// Work units of channel cc: passes of two rows, max(np2, 1) units each.
+__device__ __forceinline__ int64_t pair_units(const nlb_struct_problem& P, int cc) {
+    const nlb_channel& c = P.chan[cc];
+    return (int64_t)((c.np1 + 1) / 2) * (c.np2 > 0 ? c.np2 : 1);
+}
 
 // Per-b' record (32 floats): [0,14) (f_pp value q, same value) pairs for the
 // seven slots of the f_pp row of b'; [14], [15] the pp ladder entries of
@@ -119,29 +133,38 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_pair(nlb_struct_problem P, nlb_
     int cur_ci = -1;
     float2 x1d[NH], x2d[NH], hhd = f2(0.f, 0.f), dhd = f2(0.f, 0.f);
 
-    const int64_t t0 = (int64_t)blockIdx.x * P.n_rows / gridDim.x;
-    const int64_t t1e = (int64_t)(blockIdx.x + 1) * P.n_rows / gridDim.x;
-    int ci = t0 < t1e ? find_seg(P.row_end, P.n_channels, t0) : 0;
-    // rows of the pass starting at task t in channel cc: a0' and (two ? a0'+1 : a0')
-    auto issue = [&](int64_t t, int cc, int stage) {
+    // the block's units [w0, w1): first channel ci (units from wc), pass pi
+    int64_t W = 0;
+    for (int cc = 0; cc < P.n_channels; ++cc) W += pair_units(P, cc);
+    // (W is below 2^31: the lattice path holds a row in shared memory)
+    const int w0 = (int)((int64_t)blockIdx.x * W / gridDim.x);
+    const int w1 = (int)((int64_t)(blockIdx.x + 1) * W / gridDim.x);
+    int ci = 0, pi = 0, blo = 0, wc = 0;
+    if (w0 < w1) {
+        while (wc + pair_units(P, ci) <= w0) wc += (int)pair_units(P, ci++);
+        const int u = P.chan[ci].np2 > 0 ? P.chan[ci].np2 : 1;
+        pi = (w0 - wc) / u;
+        blo = w0 - wc - pi * u;
+    }
+    // rows 2pi and (2pi + 1, or 2pi again when alone) of channel cc
+    auto issue = [&](int cc, int pp, int stage) {
         const nlb_channel& cn = P.chan[cc];
-        const int64_t cbeg = cc ? P.row_end[cc - 1] : 0;
-        const int a0 = (int)(t - cbeg);
-        const bool tw = t + 1 < t1e && t + 1 < P.row_end[cc];
         const int rl = cn.np2 * NHP;
-        const float* s0 = B + cn.offset + (int64_t)a0 * rl;
-        pair_issue<NT>(reinterpret_cast<float*>(smem_raw + (stage ? L.st1 : L.st0)), s0, tw ? s0 + rl : s0, rl);
+        const float* s0 = B + cn.offset + (int64_t)(2 * pp) * rl;
+        pair_issue<NT>(reinterpret_cast<float*>(smem_raw + (stage ? L.st1 : L.st0)), s0,
+                       2 * pp + 1 < cn.np1 ? s0 + rl : s0, rl);
     };
-    if (t0 < t1e) issue(t0, ci, 0);
-    int pass = 0;
-    for (int64_t task = t0; task < t1e; ++pass) {
+    if (w0 < w1) issue(ci, pi, 0);
+    for (int pass = 0; w0 < w1; ++pass) {
         const int buf = pass & 1;
         const nlb_channel& ch = P.chan[ci];
-        const int64_t cbeg = ci ? P.row_end[ci - 1] : 0;
-        const bool two = task + 1 < t1e && task + 1 < P.row_end[ci];
-        const int ap0 = (int)(task - cbeg), ap1 = two ? ap0 + 1 : ap0;
+        const bool two = 2 * pi + 1 < ch.np1;
+        const int ap0 = 2 * pi, ap1 = two ? ap0 + 1 : ap0;
         const int np2 = ch.np2;
         const int rowlen = np2 * NHP;
+        const int upp = np2 > 0 ? np2 : 1;                      // units per pass
+        const int wp = wc + pi * upp;                           // first unit of this pass
+        const int bhi = w1 - wp < np2 ? w1 - wp : np2;          // b' columns [blo, bhi)
         const float2* S2 = reinterpret_cast<const float2*>(smem_raw + (buf ? L.st1 : L.st0));
 
         // per-channel tables (the block's rows are contiguous: usually unchanged)
@@ -196,7 +219,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_pair(nlb_struct_problem P, nlb_
             const double da0 = V.dpc[ch.pb1 + ap0], da1 = V.dpc[ch.pb1 + ap1];
             const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off;
             const double* pval = P.pp_val + ch.pp_col_off;
-            for (int bp = tid; bp < np2; bp += NT) {
+            for (int bp = blo + tid; bp < bhi; bp += NT) {
                 const int ab0 = ap0 * np2 + bp, ab1 = ap1 * np2 + bp;
                 float* rp = srec + bp * kPairRec;
                 rp[14] = (pptr[ab0 + 1] > pptr[ab0]) ? (float)pval[pptr[ab0]] : 0.f;
@@ -210,10 +233,15 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_pair(nlb_struct_problem P, nlb_
         __syncthreads();
         // next pass in flight while this one is worked on (its buffer was last
         // read by the pass before, which ended with a barrier)
-        const int64_t next = task + (two ? 2 : 1);
-        int next_ci = ci;
-        while (next < t1e && next >= P.row_end[next_ci] && next_ci + 1 < P.n_channels) ++next_ci;
-        if (next < t1e) issue(next, next_ci, buf ^ 1);
+        const bool more = wp + upp < w1;
+        int nci = ci, npi = pi + 1, nwc = wc;
+        if (more) {
+            while (2 * npi >= P.chan[nci].np1) {   // past the channel's last pass
+                nwc += (int)pair_units(P, nci++);
+                npi = 0;
+            }
+            issue(nci, npi, buf ^ 1);
+        }
         // Gb[k'][i'j'] = sum_c f_ck B[a'][c'][i'j'] of both rows (holes k of
         // label g2), then the T1 Fock terms F2[a'][i'] of both rows
         for (int e = tid; e < NH * NHP; e += NT) {
@@ -227,7 +255,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_pair(nlb_struct_problem P, nlb_
             sgb[e] = acc;
         }
         __syncthreads();
-        if (tid < 2 * NH && (tid < NH || two)) {
+        if (blo == 0 && tid < 2 * NH && (tid < NH || two)) {
             const int r = tid / NH, i = tid - r * NH;
             float acc = 0.f;
 #pragma unroll
@@ -237,7 +265,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_pair(nlb_struct_problem P, nlb_
             }
             F2[ch.f2_off + (int64_t)(r ? ap1 : ap0) * NH + i] = acc;
         }
-        if (active && grp < np2) {
+        if (active && blo + grp < bhi) {
             float2 gb[NH];
 #pragma unroll
             for (int k = 0; k < NH; ++k) gb[k] = sgb[k * NHP + hp];
@@ -321,22 +349,25 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_pair(nlb_struct_problem P, nlb_
             // the L2 loads of one b' step go out a step ahead of its math
             float2 nA[kLatNa], gA[3], nB[kLatNa], gB2[3];
             float g6A, g6B;
-            load(grp, nA, gA, g6A);
-            for (int bp = grp; bp < np2; bp += 2 * NB) {
+            load(blo + grp, nA, gA, g6A);
+            for (int bp = blo + grp; bp < bhi; bp += 2 * NB) {
                 const int b1 = bp + NB;
-                load(b1 < np2 ? b1 : bp, nB, gB2, g6B);
+                load(b1 < bhi ? b1 : bp, nB, gB2, g6B);
                 step(bp, nA, gA, g6A);
-                if (b1 >= np2) break;
+                if (b1 >= bhi) break;
                 const int b2 = b1 + NB;
-                load(b2 < np2 ? b2 : b1, nA, gA, g6A);
+                load(b2 < bhi ? b2 : b1, nA, gA, g6A);
                 step(b1, nB, gB2, g6B);
             }
             nrm += (double)nrm2.x;
             if (two) nrm += (double)nrm2.y;
         }
         __syncthreads();
-        task = next;
-        ci = next_ci;
+        if (!more) break;
+        ci = nci;
+        pi = npi;
+        wc = nwc;
+        blo = 0;
     }
     const double s = block_sum(nrm);
     if (threadIdx.x == 0) V.slots(kRedDt2)[blockIdx.x] = 4.0 * s;
