@@ -382,7 +382,10 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_t2_rows(nlb_struct_problem P
 // * the terms along a (f_pp neighbours of a' and the Ga rows) are read from
 //   L2 with one coalesced load per term, issued one b' step ahead; the
 //   neighbour rows of consecutive a' overlap because each block takes a
-//   contiguous range of rows.
+//   contiguous range of rows;
+// * the rows' b' columns are split evenly over the blocks, so a block may
+//   start or end inside a row (1254 rows on 148 blocks at L=6 would
+//   otherwise leave some blocks nine rows and others eight).
 //
 // Launched only when every f_pp row has at most kLatNa off-diagonal entries
 // (max_fpp_offdiag), so the f_pp row of b' with its diagonal fits the
@@ -471,22 +474,38 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
     T x1[NH], x2[NH], hh = T(0), dh = T(0);
     float2 x12[NH];   // PAIR: (x1[k], x2[k])
 
-    const int64_t t0 = (int64_t)blockIdx.x * P.n_rows / gridDim.x;
-    const int64_t t1e = (int64_t)(blockIdx.x + 1) * P.n_rows / gridDim.x;
-    int ci = t0 < t1e ? find_seg(P.row_end, P.n_channels, t0) : 0;
+    // work units: max(np2, 1) b' columns per row, rows in channel order, cut
+    // into gridDim.x equal contiguous ranges [w0, w1) (a block may start or
+    // end inside a row: it stages the row and forms Gb, updates the columns
+    // of its range, and the block holding column 0 writes the row's F2);
+    // W is below 2^31 because the lattice path holds a row in shared memory
+    int64_t W = 0;
+    for (int cc = 0; cc < P.n_channels; ++cc) W += lat_units(P, cc);
+    const int w0 = (int)((int64_t)blockIdx.x * W / gridDim.x);
+    const int w1 = (int)((int64_t)(blockIdx.x + 1) * W / gridDim.x);
+    int ci = 0, ap = 0, blo = 0, wc = 0;
+    auto issue = [&](int cc, int a, int stage) {
+        const nlb_channel& cn = P.chan[cc];
+        const int rl = cn.np2 * NHP;
+        return lat_issue_row<T, NT>(reinterpret_cast<T*>(smem_raw + (stage ? L.row1 : L.row0)),
+                                    B + cn.offset + (int64_t)a * rl, rl);
+    };
     int mis = 0;
-    if (t0 < t1e) {
-        const nlb_channel c0 = P.chan[ci];
-        const int ap0 = (int)(t0 - (ci ? P.row_end[ci - 1] : 0));
-        const int rl = c0.np2 * NHP;
-        mis = lat_issue_row<T, NT>(reinterpret_cast<T*>(smem_raw + L.row0), B + c0.offset + (int64_t)ap0 * rl, rl);
+    if (w0 < w1) {
+        while (wc + lat_units(P, ci) <= w0) wc += (int)lat_units(P, ci++);
+        const int u = P.chan[ci].np2 > 0 ? P.chan[ci].np2 : 1;
+        ap = (w0 - wc) / u;
+        blo = w0 - wc - ap * u;
+        mis = issue(ci, ap, 0);
     }
-    for (int64_t task = t0; task < t1e; ++task) {
-        const int buf = (int)((task - t0) & 1);
+    for (int pass = 0; w0 < w1; ++pass) {
+        const int buf = pass & 1;
         const nlb_channel& ch = P.chan[ci];
-        const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
         const int np2 = ch.np2;
         const int rowlen = np2 * NHP;
+        const int upp = np2 > 0 ? np2 : 1;                      // units per row
+        const int wp = wc + ap * upp;                           // first unit of this row
+        const int bhi = w1 - wp < np2 ? w1 - wp : np2;          // b' columns [blo, bhi)
         const int64_t rbase = ch.offset + (int64_t)ap * rowlen;
         // (shared addresses computed from smem_raw directly, never through a
         // pointer array, so that every access stays a shared-memory access)
@@ -553,7 +572,7 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
         const double da = V.dpc[ch.pb1 + ap];
         const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off;
         const double* pval = P.pp_val + ch.pp_col_off;
-        for (int bp = tid; bp < np2; bp += NT) {
+        for (int bp = blo + tid; bp < bhi; bp += NT) {
             const int ab = ap * np2 + bp;
             srec[bp * RW + RW - 1] = (pptr[ab + 1] > pptr[ab]) ? (T)pval[pptr[ab]] : T(0);
             sdp[bp] = (T)(da + V.dpc[ch.pb2 + bp]);
@@ -562,14 +581,14 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
         __syncthreads();
         // next row in flight while this one is worked on (its buffer was last
         // read by the row before, which ended with a barrier)
-        int next_ci = ci, next_mis = 0;
-        if (task + 1 < t1e) {
-            if (task + 1 >= P.row_end[ci]) ++next_ci;
-            const nlb_channel cn = P.chan[next_ci];
-            const int apn = (int)(task + 1 - (next_ci ? P.row_end[next_ci - 1] : 0));
-            const int rl = cn.np2 * NHP;
-            next_mis = lat_issue_row<T, NT>(reinterpret_cast<T*>(smem_raw + (buf ? L.row0 : L.row1)),
-                                            B + cn.offset + (int64_t)apn * rl, rl);
+        const bool more = wp + upp < w1;
+        int nci = ci, nap = ap + 1, nwc = wc, next_mis = 0;
+        if (more) {
+            while (nap >= P.chan[nci].np1) {   // past the channel's last row
+                nwc += (int)lat_units(P, nci++);
+                nap = 0;
+            }
+            next_mis = issue(nci, nap, buf ^ 1);
         }
         // Gb[k'][hp] = sum_c f_ck B[a'][c'][hp] (holes k of label g2), then F2
         for (int e = tid; e < NH * NHP; e += NT) {
@@ -581,13 +600,13 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
             sgb[e] = acc;
         }
         __syncthreads();
-        if (tid < NH) {
+        if (blo == 0 && tid < NH) {
             T acc = T(0);
 #pragma unroll
             for (int kq = 0; kq < NH; ++kq) acc += sgb[kq * NHP + tid * NH + kq];
             F2[ch.f2_off + (int64_t)ap * NH + tid] = acc;
         }
-        if (active && grp < np2) {
+        if (active && blo + grp < bhi) {
             const T* __restrict__ gB = B + ch.offset + hp;
             const T* __restrict__ gG = Ga + ch.ga_off + hp;    // Ga[b'][k'][i'j']: k' at stride NHP
             T* __restrict__ Bout = Bo + rbase + hp;
@@ -683,20 +702,20 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
             // the L2 loads of one b' step go out a step ahead of its math
             T rnb[kLatNa], rgv[NH];
             {
-                const int eb = grp * NHP;
+                const int eb = (blo + grp) * NHP;
 #pragma unroll
                 for (int q = 0; q < kLatNa; ++q) rnb[q] = __ldg(gB + aoff[q] + eb);
 #pragma unroll
                 for (int k = 0; k < NH; ++k) rgv[k] = __ldg(gG + eb * NH + k * NHP);
             }
-            for (int bp = grp; bp < np2; bp += NB) {
+            for (int bp = blo + grp; bp < bhi; bp += NB) {
                 const int eb = bp * NHP;
                 T nb[kLatNa], gv[NH];
 #pragma unroll
                 for (int q = 0; q < kLatNa; ++q) nb[q] = rnb[q];
 #pragma unroll
                 for (int k = 0; k < NH; ++k) gv[k] = rgv[k];
-                const int ebn = (bp + NB < np2) ? eb + NB * NHP : eb;
+                const int ebn = (bp + NB < bhi) ? eb + NB * NHP : eb;
 #pragma unroll
                 for (int q = 0; q < kLatNa; ++q) rnb[q] = __ldg(gB + aoff[q] + ebn);
 #pragma unroll
@@ -706,7 +725,11 @@ __global__ void __launch_bounds__(NT, MINB) k_t2_lat(nlb_struct_problem P, nlb_s
             nrm += (double)nrm_row;
         }
         __syncthreads();
-        ci = next_ci;
+        if (!more) break;
+        ci = nci;
+        ap = nap;
+        wc = nwc;
+        blo = 0;
         mis = next_mis;
     }
     const double s = block_sum(nrm);

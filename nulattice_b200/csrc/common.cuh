@@ -233,6 +233,14 @@ __device__ __forceinline__ T ga_element(const nlb_struct_problem& P, const T* B,
 
 __host__ __device__ inline int64_t lat_round16(int64_t b) { return (b + 15) & ~int64_t(15); }
 
+// Work units of channel cc for the row kernels that split rows by b'
+// columns: max(np2, 1) per row (a row with no columns still is one unit, so
+// that its per-row outputs get a writer).
+__device__ __forceinline__ int64_t lat_units(const nlb_struct_problem& P, int cc) {
+    const nlb_channel& c = P.chan[cc];
+    return (int64_t)c.np1 * (c.np2 > 0 ? c.np2 : 1);
+}
+
 // Asynchronous global -> shared copies (cp.async) and vector loads of
 // 16-byte aligned shared-memory records.
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {

@@ -56,7 +56,10 @@ int lcheck(const char* where) {
 // scratch layout (doubles): Y1[p*h] Z1 contributions gathered from T2 rows
 // (general path), U[h*h] = t1^T lam1, T[h*h] X_hh contractions, fc[n_t1c]
 // f_ph per label, and the lattice path's per-writer slots: Y1r[n_f2] (the Z1
-// contribution of row a' of each channel, [a'][k']), Y1c[kMaxColChunks][n_f2]
+// contribution of row a' of each channel, [a'][k'], from the block holding
+// the row's first b' column), Y1q[n_f2] (the part of the row's b' columns
+// that the next block holds, zero when one block holds the whole row),
+// Y1c[kMaxColChunks][n_f2]
 // (of column b' and one row chunk of the column pass, [b'][k']) and
 // Tp[col items][2][49] (the X_hh contractions of one column-pass block, g1
 // side then g2 side).  Every slot has exactly one writer; k_l_t1 and
@@ -78,7 +81,7 @@ __host__ __device__ inline int64_t col_items_max(const nlb_struct_problem& P) {
 // channel), and its X_hh contractions into Tg[row][side][k'][m'] (max_nh^2
 // per side); k_l_rows_reduce adds them in a fixed order into Y1 and T.
 struct LView {
-    double *Y1, *U, *T, *fc, *Y1r, *Y1c, *Tp, *Yg, *Tg;
+    double *Y1, *U, *T, *fc, *Y1r, *Y1q, *Y1c, *Tp, *Yg, *Tg;
 };
 
 __host__ __device__ inline LView lview(double* acc, const nlb_struct_problem& P) {
@@ -88,7 +91,8 @@ __host__ __device__ inline LView lview(double* acc, const nlb_struct_problem& P)
     v.T = v.U + (int64_t)P.h * P.h;
     v.fc = v.T + (int64_t)P.h * P.h;
     v.Y1r = v.fc + P.n_t1c;
-    v.Y1c = v.Y1r + P.n_f2;
+    v.Y1q = v.Y1r + P.n_f2;
+    v.Y1c = v.Y1q + P.n_f2;
     v.Tp = v.Y1c + (int64_t)kMaxColChunks * P.n_f2;
     v.Yg = v.Tp + col_items_max(P) * 2 * kLHP_;   // general path only
     v.Tg = v.Yg + P.n_t2;
@@ -417,7 +421,7 @@ __global__ void k_l_t1(nlb_struct_problem P, nlb_lambda_state S, int nchunk) {
             for (int ci = 0; ci < P.n_channels; ++ci) {
                 const nlb_channel& ch = P.chan[ci];
                 const int64_t o = ch.f2_off + (int64_t)xl * ch.nh1 + ml;
-                if (ch.g1 == g) y1 += V.Y1r[o];
+                if (ch.g1 == g) y1 += V.Y1r[o] + V.Y1q[o];
                 if (ch.g2 == g)
                     for (int cq = 0; cq < nchunk; ++cq) y1 += V.Y1c[(int64_t)cq * P.n_f2 + o];
             }
@@ -849,14 +853,29 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
     double dnrm = 0.0, lnrm = 0.0;
     int cur_ci = -1;
     T x1t[kLH], x2t[kLH], shh = T(0), dh = T(0);
-    const int64_t t0 = (int64_t)blockIdx.x * P.n_rows / gridDim.x;
-    const int64_t t1e = (int64_t)(blockIdx.x + 1) * P.n_rows / gridDim.x;
-    for (int64_t task = t0; task < t1e; ++task) {
-        const int ci = find_seg(P.row_end, P.n_channels, task);
+    // work units: np2 b' columns per row, rows in channel order, cut into
+    // gridDim.x equal contiguous ranges [w0, w1).  Every channel has np2 =
+    // np1 = np and the grid is at most the row count, so a range is at
+    // least np units long and a row lies in one block or in two consecutive
+    // ones: the first writes the row's Z1 part to Y1r, the second to Y1q.
+    int64_t W = 0;
+    for (int cc = 0; cc < P.n_channels; ++cc) W += lat_units(P, cc);
+    const int w0 = (int)((int64_t)blockIdx.x * W / gridDim.x);
+    const int w1 = (int)((int64_t)(blockIdx.x + 1) * W / gridDim.x);
+    int ci = 0, ap = 0, blo = 0, wc = 0;
+    if (w0 < w1) {
+        while (wc + lat_units(P, ci) <= w0) wc += (int)lat_units(P, ci++);
+        const int u = P.chan[ci].np2 > 0 ? P.chan[ci].np2 : 1;
+        ap = (w0 - wc) / u;
+        blo = w0 - wc - ap * u;
+    }
+    while (w0 < w1) {
         const nlb_channel& ch = P.chan[ci];
-        const int ap = (int)(task - (ci ? P.row_end[ci - 1] : 0));
         const int np2 = ch.np2;
         const int rowlen = np2 * kLHP;
+        const int upp = np2 > 0 ? np2 : 1;                      // units per row
+        const int wp = wc + ap * upp;                           // first unit of this row
+        const int bhi = w1 - wp < np2 ? w1 - wp : np2;          // b' columns [blo, bhi)
         const int64_t rbase = ch.offset + (int64_t)ap * rowlen;
         const int a = P.p_ord[ch.pb1 + ap];
         // the row, asynchronously (ragged head, 16-byte middle, ragged tail)
@@ -938,7 +957,7 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
         const double da = PV.dpc[ch.pb1 + ap];
         const int32_t* pptr = P.pp_ptr + ch.pp_ptr_off;
         const double* pval = P.pp_val + ch.pp_col_off;
-        for (int bq = tid; bq < np2; bq += NT) {
+        for (int bq = blo + tid; bq < bhi; bq += NT) {
             const int ab = ap * np2 + bq;
             srec[bq * kLRec + 15] = (pptr[ab + 1] > pptr[ab]) ? (T)pval[pptr[ab]] : T(0);
             srec[bq * kLRec + 23] = (T)(da + PV.dpc[ch.pb2 + bq]);
@@ -976,7 +995,7 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
         T acc3 = T(0);
 #pragma unroll
         for (int k = 0; k < kLH; ++k) acc_ga[k] = T(0);
-        if (active && grp < np2) {
+        if (active && blo + grp < bhi) {
             const T* __restrict__ gL = Lm + ch.offset + hp;
             const T* __restrict__ gG = Ga + ch.ga_off + hp;
             const T* __restrict__ gH = Ha + ch.ga_off + hp;
@@ -986,7 +1005,7 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
             const T* s_col = sr + jp;            // Lam[a'][b'][k'][j'] at eb + k' NH
             const T* s_row = sr + ip * kLH;      // Lam[a'][b'][i'][k'] at eb + k'
             T nrm_d = T(0), nrm_l = T(0);
-            for (int bq = grp; bq < np2; bq += NB) {
+            for (int bq = blo + grp; bq < bhi; bq += NB) {
                 const int eb = bq * kLHP;
                 T nb[kLNa], gv[kLH];
 #pragma unroll
@@ -1053,9 +1072,22 @@ __global__ void __launch_bounds__(NT, MINB) k_l_lat(nlb_struct_problem P, nlb_la
         if (tid < kLH) {
             double s = 0.0;
             for (int w = 0; w < NT / 32; ++w) s += sred[w][tid];
-            V.Y1r[ch.f2_off + (int64_t)ap * kLH + tid] = s;   // this block owns row a' of the channel
+            const int64_t o = ch.f2_off + (int64_t)ap * kLH + tid;
+            if (blo > 0) {
+                V.Y1q[o] = s;             // the rest of a row that the block before began
+            } else {
+                V.Y1r[o] = s;
+                if (bhi == np2) V.Y1q[o] = 0.0;   // the whole row is this block's
+            }
         }
         __syncthreads();
+        if (wp + upp >= w1) break;
+        ++ap;
+        while (ap >= P.chan[ci].np1) {   // past the channel's last row
+            wc += (int)lat_units(P, ci++);
+            ap = 0;
+        }
+        blo = 0;
     }
     const double s1 = block_sum(dnrm);
     const double s2 = block_sum(lnrm);
@@ -1210,7 +1242,7 @@ extern "C" {
 int64_t nlb_lambda_acc_len(const nlb_struct_problem* prob) {
     if (!prob) return 0;
     const int64_t common = (int64_t)prob->p * prob->h + 2 * (int64_t)prob->h * prob->h + prob->n_t1c +
-                           (int64_t)(1 + kMaxColChunks) * prob->n_f2 + col_items_max(*prob) * 2 * kLHP;
+                           (int64_t)(2 + kMaxColChunks) * prob->n_f2 + col_items_max(*prob) * 2 * kLHP;
     if (lattice(prob)) return common;
     // general path: the row kernel's Yg and Tg slots
     return common + prob->n_t2 + prob->n_rows * 2 * (int64_t)prob->max_nh * prob->max_nh;
