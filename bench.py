@@ -782,7 +782,8 @@ def adjoint_leg(dev):
             "t_forward_s": info2["t_forward"], "t_lambda_s": info2["t_lambda"],
             "lambda_over_forward": info2["t_lambda"] / info2["t_forward"],
             "lambda_iters": info2["lambda_iters"], "forward_iters": info2["iterations"],
-            "lambda_iters_fp32": info2.get("lambda_iters_fp32"), "lambda_path": info2.get("lambda_path")}
+            "lambda_iters_fp32": info2.get("lambda_iters_fp32"), "lambda_path": info2.get("lambda_path"),
+            "t_lambda_fp32_phase_s": info2.get("t_lambda_fp32"), "t_lambda_fp64_phase_s": info2.get("t_lambda_fp64")}
 
 
 def e2e_leg(args, fock, two, dev):

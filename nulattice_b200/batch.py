@@ -174,7 +174,7 @@ class _Instance:
         self.l32 = lam_buffers(torch.float32, own_t2=True) if self.lattice else None
         self.out = torch.zeros(8, **f64)
         solver = _adj.LambdaSolver(eng)
-        self.dw_dv = [solver.coefficients(prob.dv[2]), solver.coefficients(prob.dw[2])]
+        self.dw_dv = [solver.coefficients(prob.dv[1], prob.dv[2])[:2], solver.coefficients(prob.dw[1], prob.dw[2])[:2]]
 
     def lambda_state(self, b, dtype, fwd, ring):
         st = _lib.LambdaState()
@@ -256,8 +256,8 @@ class BatchScan:
             o = x.out.cpu().numpy()
             pl = x.eng.plan
             p, h = pl.p, pl.h
-            acc = x.l64["acc"].cpu().numpy()
-            UT = acc[p * h:p * h + h * h].reshape(h, h) + acc[p * h + h * h:p * h + 2 * h * h].reshape(h, h)
+            ut = x.l64["acc"][p * h:p * h + 2 * h * h].cpu().numpy()   # U and T only
+            UT = ut[:h * h].reshape(h, h) + ut[h * h:].reshape(h, h)
             grads = []
             ok = int(o[5]) == 1   # the Lambda equations converged (the forward solve did, too)
             for d, part in enumerate((x.prob.dv, x.prob.dw)):

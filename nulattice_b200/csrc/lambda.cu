@@ -513,18 +513,37 @@ __global__ void k_l_coupling(nlb_struct_problem P, nlb_lambda_state S, const dou
     const double* t2 = static_cast<const double*>(S.t2);
     const PrepView PV = prep_view(S.prep, P);
     double acc = 0.0;
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < P.n_t2; u += (int64_t)gridDim.x * blockDim.x) {
-        const int ci = find_seg(P.t2_end, P.n_channels, u);
-        const nlb_channel& ch = P.chan[ci];
-        const int64_t loc = u - ch.offset;
-        const int nhp = ch.nh1 * ch.nh2;
-        const int hp = (int)(loc % nhp);
-        const int ab = (int)(loc / nhp);
-        const int ap = ab / ch.np2, bp = ab - ap * ch.np2;
-        const int ip = hp / ch.nh2, jp = hp - ip * ch.nh2;
-        const double tau = t2[u] + PV.t1c[P.t1c_base[ch.g1] + ap * ch.nh1 + ip] *
-                                       PV.t1c[P.t1c_base[ch.g2] + bp * ch.nh2 + jp];
-        acc += Lm[u] * (dw[ch.hh_ptr_off + hp] + dv[ch.pp_ptr_off + ab]) * tau;
+    // the block's contiguous range [u0, u1) of the compact amplitudes; a
+    // thread walks it at stride blockDim.x, tracking its channel, row a' and
+    // element e of the row (no per-element search or 64-bit division)
+    const int64_t u0 = (int64_t)blockIdx.x * P.n_t2 / gridDim.x;
+    const int64_t u1 = (int64_t)(blockIdx.x + 1) * P.n_t2 / gridDim.x;
+    int64_t u = u0 + threadIdx.x;
+    if (u < u1) {
+        int ci = find_seg(P.t2_end, P.n_channels, u);
+        const nlb_channel* ch = &P.chan[ci];
+        int nhp = ch->nh1 * ch->nh2, rowlen = ch->np2 * nhp;
+        int ap = (int)((u - ch->offset) / rowlen);
+        int e = (int)(u - ch->offset - (int64_t)ap * rowlen);
+        for (; u < u1; u += blockDim.x, e += blockDim.x) {
+            while (e >= rowlen) {   // next row, or the first row of a later channel
+                e -= rowlen;
+                if (++ap >= ch->np1) {
+                    do {
+                        ch = &P.chan[++ci];
+                    } while ((int64_t)ch->np1 * ch->np2 * ch->nh1 * ch->nh2 == 0);   // channels hold
+                    // their amplitudes back to back, so u is the first one of this channel
+                    nhp = ch->nh1 * ch->nh2;
+                    rowlen = ch->np2 * nhp;
+                    ap = 0;
+                }
+            }
+            const int bp = e / nhp, hp = e - bp * nhp;
+            const int ip = hp / ch->nh2, jp = hp - ip * ch->nh2;
+            const double tau = t2[u] + PV.t1c[P.t1c_base[ch->g1] + ap * ch->nh1 + ip] *
+                                           PV.t1c[P.t1c_base[ch->g2] + bp * ch->nh2 + jp];
+            acc += Lm[u] * (dw[ch->hh_ptr_off + hp] + dv[ch->pp_ptr_off + ap * ch->np2 + bp]) * tau;
+        }
     }
     const double s = block_sum(acc);
     if (threadIdx.x == 0) PV.slots(0)[blockIdx.x] = s;
