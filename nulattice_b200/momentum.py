@@ -263,24 +263,57 @@ def jacobi_gap(eng, t2):
 
 def _iterate(eng, xs, cur, eps, maxSteps, max_diis, mixing, criterion, verbose, step0=0):
     """The solver loop on engine ``eng`` from the amplitudes ``xs[cur]``.
-    Returns (E, cur, status, steps)."""
+    Returns (E, cur, status, steps).
+
+    The energy of each step comes back through a page-locked slot and an
+    event, and the next step is queued before that energy is read, so the
+    device does not wait for the host's convergence test.  Only a step after
+    which a DIIS extrapolation is due waits for its test first (the
+    extrapolation rewrites the amplitudes in place).  A step queued after
+    the converged one writes the buffer of the step before, so the converged
+    amplitudes stay untouched; the steps, and so the results, are the same
+    as with a test after every step."""
     L, sp = eng.L, eng.sp
     n = eng.plan.n_t2
     use_diis = criterion == "soa" and max_diis > 0
     if use_diis:
-        err = torch.zeros((max_diis, n), dtype=eng.dtype, device=eng.dev)
-        hist = torch.zeros((max_diis, n), dtype=eng.dtype, device=eng.dev)
+        # every error / history row is written before an extrapolation reads it
+        err = torch.empty((max_diis, n), dtype=eng.dtype, device=eng.dev)
+        hist = torch.empty((max_diis, n), dtype=eng.dtype, device=eng.dev)
         work = torch.zeros(_lib.NLB_DENSE_WORK_DOUBLES, dtype=torch.float64, device=eng.dev)
         diis = L.nlb_vec_diis_f32 if eng.f32 else L.nlb_vec_diis_f64
-        nerr = 0
+    nerr = 0
+    if getattr(eng, "_host_e", None) is None:   # page-locked energy slots, kept on the engine
+        eng._host_e = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+        eng._events = [torch.cuda.Event(), torch.cuda.Event()]
+    host_e, events = eng._host_e, eng._events
+
+    def launch(k, src, e_slot):
+        """Step k from xs[src] into xs[src ^ 1] (DIIS error into err[e_slot]),
+        its energy, and the energy's copy into host slot k % 2."""
+        eng.step(xs[src], xs[src ^ 1], err[e_slot] if use_diis else None, mixing)
+        eng.energy(xs[src ^ 1])
+        with torch.cuda.stream(eng.stream):
+            host_e[k % 2:k % 2 + 1].copy_(eng.bufs["energy"], non_blocking=True)
+            events[k % 2].record(eng.stream)
+
     prev = float(eng.energy(xs[cur]).item())
     if verbose and step0 == 0:
         print(f"Step 0: {prev}")
     status, e, it = "max_iter", prev, 0
+    if maxSteps >= 1:
+        launch(1, cur, nerr)
     for it in range(1, maxSteps + 1):
-        eng.step(xs[cur], xs[cur ^ 1], err[nerr] if use_diis else None, mixing)
+        # step `it` (xs[cur] -> xs[cur ^ 1]) is queued; queue step it + 1
+        # unless a DIIS extrapolation would come between them
+        ahead = it < maxSteps and (not use_diis or nerr + 1 < max_diis)
+        if ahead:
+            if use_diis:
+                hist[nerr].copy_(xs[cur ^ 1])
+            launch(it + 1, cur ^ 1, nerr + 1 if use_diis else 0)
+        events[it % 2].synchronize()
+        e = float(host_e[it % 2])
         cur ^= 1
-        e = float(eng.energy(xs[cur]).item())
         if verbose:
             print(f"Step {step0 + it}: {e}", "difference =", abs(e - prev) / abs(e) if e != 0 else float("inf"))
         if criterion == "soa":
@@ -291,7 +324,8 @@ def _iterate(eng, xs, cur, eps, maxSteps, max_diis, mixing, criterion, verbose, 
             status = "converged"
             break
         if use_diis:
-            hist[nerr].copy_(xs[cur])
+            if not ahead:
+                hist[nerr].copy_(xs[cur])
             nerr += 1
             if nerr == max_diis:
                 _lib.check(diis(err.data_ptr(), hist.data_ptr(), n, max_diis, work.data_ptr(), xs[cur].data_ptr(),
@@ -303,6 +337,8 @@ def _iterate(eng, xs, cur, eps, maxSteps, max_diis, mixing, criterion, verbose, 
             status = "diverged"
             break
         prev = e
+        if not ahead and it < maxSteps:
+            launch(it + 1, cur, nerr)
     return e, cur, status, it
 
 
