@@ -77,6 +77,16 @@ def _coo(block):
     return uniq[keep], acc[keep]
 
 
+def _csr_ptr(rows, n):
+    """CSR row pointer (length n + 1, int64) of the sorted or unsorted row
+    indices ``rows`` in [0, n): one count and one running sum, written in
+    place."""
+    ptr = np.empty(n + 1, np.int64)
+    ptr[0] = 0
+    np.cumsum(np.bincount(rows, minlength=n), out=ptr[1:])
+    return ptr
+
+
 def _nonzero2(a):
     """``np.nonzero`` of a 2-D float array (same indices, same row-major
     order, -0.0 counted as zero and NaN as non-zero), through a flat scan
@@ -275,14 +285,14 @@ def detect(fock_mats, two_body_int, t1initial=None):
     r, c = p_pos[fpp_r], p_pos[fpp_c]
     order = np.argsort(r * max(p, 1) + c, kind="stable")
     r, c = r[order], c[order]
-    fpp_ptr = np.concatenate(([0], np.cumsum(np.bincount(r, minlength=p)))).astype(np.int64)
+    fpp_ptr = _csr_ptr(r, p)
     fpp_col = (c - p_base[p_label[p_ord[c]]]).astype(np.int64)
     fpp_val = np.ascontiguousarray(f_pp[fpp_r[order], fpp_c[order]], dtype=np.float64)
     # f_ph per hole (label-ordered holes, label-local particle rows)
     r, c = h_pos[fph_c], p_pos[fph_r]
     order = np.argsort(r * max(p, 1) + c, kind="stable")
     r, c = r[order], c[order]
-    fph_ptr = np.concatenate(([0], np.cumsum(np.bincount(r, minlength=h)))).astype(np.int64)
+    fph_ptr = _csr_ptr(r, h)
     fph_col = (c - p_base[p_label[p_ord[c]]]).astype(np.int64)
     fph_val = np.ascontiguousarray(f_ph[fph_r[order], fph_c[order]], dtype=np.float64)
 
@@ -299,7 +309,7 @@ def detect(fock_mats, two_body_int, t1initial=None):
         else:
             out = inp = np.zeros(0, np.int64); vv = np.zeros(0)
         order = np.argsort(out, kind="stable")
-        hh_ptr.append(np.concatenate(([0], np.cumsum(np.bincount(out, minlength=ch.nh1 * ch.nh2)))).astype(np.int64))
+        hh_ptr.append(_csr_ptr(out, ch.nh1 * ch.nh2))
         hh_col.append(inp[order].astype(np.int64)); hh_val.append(vv[order])
         # particle-particle: output (a,b) in (g1,g2), input (c,d) in (g1,g2)
         if len(pp_idx):
@@ -311,7 +321,7 @@ def detect(fock_mats, two_body_int, t1initial=None):
         else:
             out = inp = np.zeros(0, np.int64); vv = np.zeros(0)
         order = np.argsort(out, kind="stable")
-        pp_ptr.append(np.concatenate(([0], np.cumsum(np.bincount(out, minlength=ch.np1 * ch.np2)))).astype(np.int64))
+        pp_ptr.append(_csr_ptr(out, ch.np1 * ch.np2))
         pp_col.append(inp[order].astype(np.int64)); pp_val.append(vv[order])
 
     plan = ChannelPlan(p=p, h=h, n_labels=G, p_label=p_label, h_label=h_label, p_loc=p_loc,
